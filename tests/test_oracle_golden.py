@@ -1,0 +1,179 @@
+"""Pins the CPU oracle to massively's own known answers (CPU only).
+
+Every vector in tests/golden/known_answers.py comes from a massively test or
+doctest; the oracle must reproduce each one before any GPU result is judged
+against it.
+"""
+import numpy as np
+import pytest
+
+from tests.golden import known_answers as K
+
+
+def test_scan_known_answers(orc):
+    for case in K.SCAN:
+        if case["kind"] == "inclusive":
+            got = orc.inclusive_scan(case["x"], case["op"])
+        else:
+            got = orc.exclusive_scan(case["x"], case["op"], case["init"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+
+
+def test_scan_boundary_probes(orc):
+    ones = np.ones(K.SCAN_ONES["n"], np.uint32)
+    inc = orc.inclusive_scan(ones, "add")
+    for i, v in K.SCAN_ONES["probes"].items():
+        assert inc[i] == v
+    exc = orc.exclusive_scan(ones, "add", K.SCAN_EXCL_ONES["init"])
+    for i in K.SCAN_EXCL_ONES["probes"]:
+        assert exc[i] == K.SCAN_EXCL_ONES["init"] + i
+    tl = orc.exclusive_scan(np.ones(K.SCAN_TAKE_LEFT["n"], np.uint32), "take_left",
+                            K.SCAN_TAKE_LEFT["init"])
+    assert (tl == K.SCAN_TAKE_LEFT["want"]).all()
+
+
+def test_reduce_known_answers(orc):
+    for case in K.REDUCE:
+        assert orc.reduce(case["x"], case["op"], case["init"]) == case["want"], case["src"]
+
+
+def test_selection_known_answers(orc):
+    for case in K.SELECT:
+        fn = orc.copy_where if case["kind"] == "copy_where" else orc.remove_where
+        np.testing.assert_array_equal(fn(case["x"], case["stencil"]), case["want"],
+                                      err_msg=case["src"])
+    rows = K.COPY_WHERE_ROWS
+    got = orc.copy_where(rows["cols"], rows["stencil"])
+    for g, w in zip(got, rows["want"]):
+        np.testing.assert_array_equal(g, w)
+    sp = K.STENCIL_POSITIONS
+    np.testing.assert_array_equal(orc.inclusive_scan(orc.flags(sp["stencil"], "is_true"), "add"),
+                                  sp["want"])
+    for case in K.PARTITION:
+        out, b = orc.partition(case["x"], case["pred"])
+        assert b == case["boundary"], case["src"]
+        np.testing.assert_array_equal(out, case["want"], err_msg=case["src"])
+
+
+def test_gather_scatter_known_answers(orc):
+    for case in K.GATHER:
+        got = orc.gather(case["values"], case["idx"], case["stencil"], case["out"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+    for case in K.SCATTER:
+        got = orc.scatter(case["values"], case["idx"], case["out"], case["stencil"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+
+
+def test_ordering_known_answers(orc):
+    for case in K.SORT:
+        np.testing.assert_array_equal(orc.sort(case["x"]), case["want"], err_msg=case["src"])
+    for case in K.SORT_BY_KEY:
+        _, v = orc.sort_by_key(case["keys"], case["values"])
+        np.testing.assert_array_equal(v, case["want"], err_msg=case["src"])
+    for case in K.RADIX:
+        got = orc.radix_sort_by_key(case["keys"], case["values"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+    for case in K.RADIX_INTEGER_EXTREMES + K.RADIX_FLOAT_TOTAL_ORDER:
+        np.testing.assert_array_equal(orc.radix_perm([case["keys"]]), case["want"],
+                                      err_msg=case["src"])
+    c = K.RADIX_COMPOUND
+    np.testing.assert_array_equal(orc.radix_perm(c["keys"]), c["want"], err_msg=c["src"])
+    n = K.RADIX_513["n"]
+    keys = ((np.arange(n) * 37) % 11).astype(np.uint32)
+    got = orc.radix_sort_by_key([keys], np.arange(n, dtype=np.uint32))
+    np.testing.assert_array_equal(got, np.argsort(keys, kind="stable"))
+
+
+def test_by_key_known_answers(orc):
+    for case in K.BY_KEY:
+        if case["kind"] == "reduce":
+            k, v = orc.reduce_by_key(case["keys"], case["values"], "add", case["init"])
+            np.testing.assert_array_equal(k, case["want_keys"])
+            np.testing.assert_array_equal(v, case["want"])
+            k2, v2 = orc.reduce_by_key_literal_u32(case["keys"], case["values"], "add",
+                                                   case["init"])
+            np.testing.assert_array_equal(k2, k)
+            np.testing.assert_array_equal(v2, v)
+        else:
+            got = orc.scan_by_key(case["keys"], case["values"], "add",
+                                  exclusive=case["kind"] == "exclusive", init=case["init"])
+            np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+    s = K.BY_KEY_SEVEN
+    n = s["n"]
+    keys = np.where(np.arange(n) < 300, 1, 2).astype(np.uint32)
+    cols = [np.full(n, c, np.uint32) for c in range(1, 8)]
+    inc = [orc.scan_by_key(keys, col, "add") for col in cols]
+    assert (inc[0][299], inc[0][300], inc[0][599]) == (300, 1, 300)
+    assert (inc[6][299], inc[6][300], inc[6][599]) == (2100, 7, 2100)
+    exc = orc.scan_by_key(keys, cols[0], "add", exclusive=True, init=s["inits"][0])
+    assert (exc[0], exc[1], exc[300], exc[301]) == (10, 11, 10, 11)
+    k, vals = orc.reduce_by_key(keys, cols, ["add"] * 7, s["inits"])
+    np.testing.assert_array_equal(k, [1, 2])
+    np.testing.assert_array_equal(vals[0], [310, 310])
+    np.testing.assert_array_equal(vals[6], [2170, 2170])
+
+
+def test_merge_and_set_known_answers(orc):
+    for case in K.MERGE:
+        np.testing.assert_array_equal(orc.merge(case["left"], case["right"]), case["want"])
+    m = K.MERGE_BY_KEY
+    _, v = orc.merge_by_key(m["lk"], m["lv"], m["rk"], m["rv"])
+    np.testing.assert_array_equal(v, m["want"])
+    for case in K.SETS:
+        np.testing.assert_array_equal(orc.set_union(case["left"], case["right"]), case["union"])
+        np.testing.assert_array_equal(orc.set_intersection(case["left"], case["right"]),
+                                      case["intersection"])
+        np.testing.assert_array_equal(orc.set_difference(case["left"], case["right"]),
+                                      case["difference"])
+    for case in K.UNIQUE:
+        np.testing.assert_array_equal(orc.unique(case["x"]), case["want"])
+
+
+def test_seg_known_answers(orc):
+    for case in K.SEG:
+        if case["kind"] == "reduce":
+            got = orc.seg_reduce(case["x"], case["offsets"], case["op"], case["init"])
+        else:
+            got = orc.seg_exclusive_scan(case["x"], case["offsets"], case["op"], case["init"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+    for case in K.SEGMENTATION:
+        off = np.concatenate([[0], np.cumsum(case["lengths"], dtype=np.uint64)]).astype(np.uint32)
+        np.testing.assert_array_equal(off, case["offsets"])
+        assert orc.validate_offsets(off) == off[-1]
+    for bad in K.INVALID_OFFSETS["cases"]:
+        assert orc.validate_offsets(bad) is None
+
+
+def test_rng_streams_are_pcg(orc):
+    # random.rs:12-22: the hash and seed key of the host restatement.
+    x = 12345
+    state = (x * 747796405 + 2891336453) & 0xFFFFFFFF
+    word = (((state >> ((state >> 28) + 4)) ^ state) * 277803737) & 0xFFFFFFFF
+    assert orc.pcg_hash32(x) == ((word >> 22) ^ word)
+    a = orc.uniform_u32(10, 20, 123, 64)
+    assert ((a >= 10) & (a <= 20)).all()
+    np.testing.assert_array_equal(a, orc.uniform_u32(10, 20, 123, 64))
+    assert not np.array_equal(a, orc.uniform_u32(10, 20, 124, 64))
+    # random_uses_generic_taken_and_tracks_nested_slice_offsets (random.rs tests)
+    full = orc.uniform_u32(10, 20, 123, 16)
+    np.testing.assert_array_equal(orc.uniform_u32(10, 20, 123, 4, offset=5), full[5:9])
+    assert not np.array_equal(orc.uniform_u32(0, 0xFFFFFFFF, 7, 64),
+                              orc.uniform_u32(0, 0xFFFFFFFF, 7 | (1 << 32), 64))
+    assert (orc.uniform_u32(4, 4, 1, 8) == 4).all()
+    u = orc.uniform_u64(1000, 2000, 777, 32)
+    assert ((u >= 1000) & (u <= 2000)).all()
+    z = orc.normal_f32(0, 1 << 16)
+    assert np.isfinite(z).all() and abs(z.mean()) < 0.02 and abs(z.std() - 1) < 0.02
+
+
+@pytest.mark.parametrize("n", K.ORACLE_LENGTHS)
+def test_oracle_agrees_with_numpy(orc, n):
+    # Independent cross-check of the oracle loops on the boundary lengths.
+    x = orc.uniform_u32(0, 0xFFFFFFFF, n + 1, n)
+    np.testing.assert_array_equal(orc.inclusive_scan(x, "add"),
+                                  np.cumsum(x, dtype=np.uint64).astype(np.uint32))
+    assert orc.reduce(x.astype(np.uint64), "add", 0) == int(x.astype(np.uint64).sum())
+    keys = x % 13
+    np.testing.assert_array_equal(orc.sort_perm(keys), np.argsort(keys, kind="stable"))
+    st = orc.flags(x, "is_even")
+    np.testing.assert_array_equal(orc.copy_where(x, st), x[st.astype(bool)])
