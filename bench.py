@@ -1,0 +1,577 @@
+"""Benchmark of the massively primitive path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--no-e2e] [--no-cpu] [--no-secondary]
+
+Default workload: the large-vector configuration of massively's north-star
+benchmark -- stable radix sort_by_key of 2^28 (u32 key, u32 value) pairs,
+keys uniform 32-bit from massively's PCG stream (seed 0), values = index.
+`value` is whole-job Gkeys/s with inputs resident in HBM; `e2e` is the same
+metric through the public API with pinned host buffers and the host<->device
+copies inside the timed region.  The other large-vector entries (u32 scan of
+2^30, f32 scan of 2^28, copy_where of 2^28, 16-bit-key sort, u64 sort of
+2^27) are measured in the same run and reported under `secondary`.
+
+Multi-GPU (torchrun): every rank runs an independent replica on its own GPU
+(the path has no exchange step); timing is the max over ranks and `value`
+counts all ranks' keys.  `--impl reference` times the CPU oracle (the
+sequential restatement of massively's own CPU reference) on rank 0 on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# DRAM traffic per launch of each workload's dominant kernel from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum), scaled to a full
+# launch; see profiles/ for the capture commands and figures.  None until
+# captured.
+NCU_TRAFFIC_BYTES = {}
+
+
+# ------------------------------------------------------------- workloads --
+
+class Workload:
+    name = ""
+    metric = ""
+    unit = ""
+    dtype = ""
+    kernel = ""
+
+    def units(self) -> float:  # keys (or bytes) per step
+        raise NotImplementedError
+
+    def alg_bytes(self) -> float:
+        raise NotImplementedError
+
+    def value_from_ms(self, ms: float, n_gpus: int) -> float:
+        raise NotImplementedError
+
+
+class SortPairsU32(Workload):
+    """Stable radix sort_by_key of (u32 key, u32 value) pairs, 8-bit onesweep
+    byte model n * (4 + 2 * P * (4 + 4)), P = 4 digit passes (68 B/pair)."""
+
+    kernel = "radix_onesweep"
+
+    def __init__(self, n=1 << 28, key_hi=0xFFFFFFFF, seed=0, tag=""):
+        self.n, self.key_hi, self.seed = n, key_hi, seed
+        bits = 32 if key_hi == 0xFFFFFFFF else int(key_hi).bit_length()
+        self.passes = 4
+        self.name = f"sort_by_key_u32_u32_2^{int(np.log2(n))}{tag}"
+        self.metric = "sort_by_key Gkeys/s"
+        self.unit = "Gkeys/s"
+        self.dtype = "u32"
+        self.bits = bits
+
+    def setup(self, ex):
+        from massively_b200 import lazy
+        import massively_b200 as mb
+        from massively_b200 import _native as N
+        self.keys = ex.alloc(np.uint32, self.n)
+        mb.runtime.check(N.lib().mb_random_uniform_u32(ex.handle, 0, self.key_hi, self.seed, 0,
+                                                      self.keys.to_col()))
+        self.vals = ex.alloc(np.uint32, self.n)
+        from massively_b200 import vector
+        vector.copy(ex, lazy.counting(0).take(self.n), self.vals)
+        self.ko = ex.alloc(np.uint32, self.n)
+        self.vo = ex.alloc(np.uint32, self.n)
+
+    def step(self, ex):
+        import ctypes as C
+        from massively_b200 import _native as N
+        from massively_b200.runtime import check
+        ks, vs = self.keys.to_src(), self.vals.to_src()
+        check(N.lib().mb_radix_sort_by_key(ex.handle, C.byref(ks), 1, C.byref(vs), 1,
+                                           C.byref(self.vo.to_col()), C.byref(self.ko.to_col())))
+
+    def units(self):
+        return float(self.n)
+
+    def alg_bytes(self):
+        return self.n * (4 + 2 * 4 * (4 + 4))
+
+    def value_from_ms(self, ms, n_gpus):
+        return self.n * n_gpus / (ms * 1e-3) / 1e9
+
+    def e2e(self, ex, host_k, host_v, out_v):
+        from massively_b200 import vector
+        dk = ex.to_device_pinned(host_k)
+        dv = ex.to_device_pinned(host_v)
+        sk, sv = vector.radix_sort_pairs(ex, dk, dv)
+        ex.copy_to_pinned(sv, out_v)
+
+    def host_inputs(self):
+        from oracle import oracle as orc
+        k = orc.uniform_u32(0, self.key_hi, self.seed, self.n)
+        v = np.arange(self.n, dtype=np.uint32)
+        return k, v
+
+    def cpu(self, sample):
+        from oracle import oracle as orc
+        k = orc.uniform_u32(0, self.key_hi, self.seed, sample)
+        v = np.arange(sample, dtype=np.uint32)
+        t = time.perf_counter()
+        orc.radix_sort_by_key([k], v)
+        return time.perf_counter() - t, sample
+
+    cpu_sample = 1 << 22
+
+
+class ScanU32(Workload):
+    """inclusive_scan (wrapping add) of 2^30 u32; bytes n * (4 + 4)."""
+
+    kernel = "scan_kernel"
+
+    def __init__(self, n=1 << 30, seed=3):
+        self.n, self.seed = n, seed
+        self.name = f"inclusive_scan_u32_2^{int(np.log2(n))}"
+        self.metric = "inclusive_scan GB/s"
+        self.unit = "GB/s"
+        self.dtype = "u32"
+
+    def setup(self, ex):
+        import massively_b200 as mb
+        from massively_b200 import _native as N
+        self.x = ex.alloc(np.uint32, self.n)
+        mb.runtime.check(N.lib().mb_random_uniform_u32(ex.handle, 0, 0xFFFFFFFF, self.seed, 0,
+                                                      self.x.to_col()))
+        self.y = ex.alloc(np.uint32, self.n)
+
+    def step(self, ex):
+        import ctypes as C
+        from massively_b200 import _native as N
+        from massively_b200.runtime import check
+        s = self.x.to_src()
+        check(N.lib().mb_inclusive_scan(ex.handle, C.byref(s), 0, self.y.to_col()))
+
+    def units(self):
+        return self.alg_bytes()
+
+    def alg_bytes(self):
+        return self.n * 8.0
+
+    def value_from_ms(self, ms, n_gpus):
+        return self.alg_bytes() * n_gpus / (ms * 1e-3) / 1e9
+
+    def host_inputs(self):
+        from oracle import oracle as orc
+        return (orc.uniform_u32(0, 0xFFFFFFFF, self.seed, self.n),)
+
+    def e2e(self, ex, host_x, out_y):
+        from massively_b200 import op, vector
+        dx = ex.to_device_pinned(host_x)
+        y = vector.inclusive_scan(ex, dx, op.Add)
+        ex.copy_to_pinned(y, out_y)
+
+    def cpu(self, sample):
+        from oracle import oracle as orc
+        x = orc.uniform_u32(0, 0xFFFFFFFF, self.seed, sample)
+        t = time.perf_counter()
+        orc.inclusive_scan(x, "add")
+        return time.perf_counter() - t, sample * 8.0
+
+    cpu_sample = 1 << 26
+
+
+class ScanF32(ScanU32):
+    """inclusive_scan (add) of 2^28 f32 N(0,1) (host Box-Muller bytes)."""
+
+    def __init__(self, n=1 << 28, seed=4):
+        super().__init__(n, seed)
+        self.name = f"inclusive_scan_f32_2^{int(np.log2(n))}"
+        self.dtype = "f32"
+
+    def setup(self, ex):
+        from oracle import oracle as orc
+        self.x = ex.to_device(orc.normal_f32(self.seed, self.n))
+        self.y = ex.alloc(np.float32, self.n)
+
+    def cpu(self, sample):
+        from oracle import oracle as orc
+        x = orc.normal_f32(self.seed, sample)
+        t = time.perf_counter()
+        orc.inclusive_scan(x, "add")
+        return time.perf_counter() - t, sample * 8.0
+
+
+class CopyWhereU32(Workload):
+    """copy_where of 2^28 u32 with the fused predicate key & 1 == 0 (~50%
+    kept); bytes n * 4 + kept * 4."""
+
+    kernel = "select_kernel"
+
+    def __init__(self, n=1 << 28, seed=5):
+        self.n, self.seed = n, seed
+        self.name = f"copy_where_u32_2^{int(np.log2(n))}"
+        self.metric = "copy_where GB/s"
+        self.unit = "GB/s"
+        self.dtype = "u32"
+
+    def setup(self, ex):
+        import massively_b200 as mb
+        from massively_b200 import _native as N
+        self.x = ex.alloc(np.uint32, self.n)
+        mb.runtime.check(N.lib().mb_random_uniform_u32(ex.handle, 0, 0xFFFFFFFF, self.seed, 0,
+                                                      self.x.to_col()))
+        self.y = ex.alloc(np.uint32, self.n)
+        import torch
+        self.cnt = torch.zeros(1, dtype=torch.uint32, device=self.x.tensor.device)
+        from oracle import oracle as orc
+        kept = int(((orc.uniform_u32(0, 0xFFFFFFFF, self.seed, min(self.n, 1 << 22)) & 1) == 0)
+                   .mean() * self.n)
+        self.kept = kept
+
+    def step(self, ex):
+        import ctypes as C
+        from massively_b200 import _native as N
+        from massively_b200.runtime import check
+        s = self.x.to_src()
+        st = self.x.to_src()
+        st.map, st.vtype = 3, 2  # IS_EVEN -> u32 flag
+        check(N.lib().mb_copy_where(ex.handle, C.byref(s), 1, C.byref(st),
+                                    C.byref(self.y.to_col()),
+                                    C.cast(C.c_void_p(self.cnt.data_ptr()),
+                                           C.POINTER(C.c_uint32)), None))
+
+    def units(self):
+        return self.alg_bytes()
+
+    def alg_bytes(self):
+        return self.n * 4.0 + self.kept * 4.0
+
+    def value_from_ms(self, ms, n_gpus):
+        return self.alg_bytes() * n_gpus / (ms * 1e-3) / 1e9
+
+
+class SortU64(Workload):
+    """Keys-only radix sort of 2^27 u64 (uniform 64-bit, seed 2); 8-bit
+    onesweep byte model n * (8 + 2 * 8 * 8) = 136 B/key."""
+
+    kernel = "radix_onesweep"
+
+    def __init__(self, n=1 << 27, seed=2):
+        self.n, self.seed = n, seed
+        self.name = f"sort_u64_2^{int(np.log2(n))}"
+        self.metric = "sort Gkeys/s"
+        self.unit = "Gkeys/s"
+        self.dtype = "u64"
+
+    def setup(self, ex):
+        import massively_b200 as mb
+        from massively_b200 import _native as N
+        self.keys = ex.alloc(np.uint64, self.n)
+        mb.runtime.check(N.lib().mb_random_uniform_u64(ex.handle, 0, 0xFFFFFFFFFFFFFFFF,
+                                                      self.seed, 0, self.keys.to_col()))
+        self.ko = ex.alloc(np.uint64, self.n)
+
+    def step(self, ex):
+        import ctypes as C
+        from massively_b200 import _native as N
+        from massively_b200.runtime import check
+        ks = self.keys.to_src()
+        check(N.lib().mb_sort(ex.handle, C.byref(ks), 0, self.ko.to_col()))
+
+    def units(self):
+        return float(self.n)
+
+    def alg_bytes(self):
+        return self.n * (8 + 2 * 8 * 8)
+
+    def value_from_ms(self, ms, n_gpus):
+        return self.n * n_gpus / (ms * 1e-3) / 1e9
+
+
+WORKLOADS = {
+    "sort_pairs_u32": lambda: SortPairsU32(),
+    "sort_pairs_u32_16bit": lambda: SortPairsU32(key_hi=65535, seed=1, tag="_keys2^16"),
+    "scan_u32": lambda: ScanU32(),
+    "scan_f32": lambda: ScanF32(),
+    "copy_where_u32": lambda: CopyWhereU32(),
+    "sort_u64": lambda: SortU64(),
+}
+SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64"]
+
+
+# -------------------------------------------------------------- helpers --
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, reasons)."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.lines = device, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_steps(ex, wl, steps, warmup, dist):
+    import torch
+    for _ in range(warmup):
+        wl.step(ex)
+    torch.cuda.synchronize()
+    if dist:
+        import torch.distributed as D
+        D.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        wl.step(ex)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ex.sync()
+    if dist:
+        import torch.distributed as D
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        D.all_reduce(t, op=D.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def cpu_baseline(wl, budget_s=12.0):
+    """The oracle on a bounded sample, repeated to ~budget_s of CPU work."""
+    total_t, total_units, reps = 0.0, 0.0, 0
+    sample = wl.cpu_sample
+    while total_t < budget_s and reps < 50:
+        t, u = wl.cpu(sample)
+        total_t += t
+        total_units += u
+        reps += 1
+    if wl.unit == "Gkeys/s":
+        v = total_units / total_t / 1e9
+    else:
+        v = total_units / total_t / 1e9
+    return {"value": v, "unit": wl.unit, "cores": 1, "kind": "port",
+            "sample": f"{reps} x {sample} items of the same workload on 1 host core "
+                      f"({os.cpu_count()} present); oracle/oracle.cpp, sequential, g++ -O3"}
+
+
+def e2e_measure(ex, wl, steps):
+    """Public API with pinned host buffers; copies inside the timed region."""
+    import torch
+    if not hasattr(wl, "e2e"):
+        return None
+    host = wl.host_inputs()
+    pinned = [torch.from_numpy(h.view(np.uint8)).pin_memory() for h in host]
+    hv = [p.numpy().view(h.dtype) for p, h in zip(pinned, host)]
+    out = torch.empty(host[-1].nbytes, dtype=torch.uint8).pin_memory()
+    out_np = out.numpy().view(host[-1].dtype)
+    wl.e2e(ex, *hv, out_np)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        wl.e2e(ex, *hv, out_np)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = sum(h.nbytes for h in host)
+    d2h = host[-1].nbytes
+    return {"value": wl.value_from_ms(dt * 1e3, 1), "unit": wl.unit,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    torch.cuda.set_device(local)
+    if dist:
+        import datetime
+
+        import torch.distributed as D
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                             device_id=torch.device(f"cuda:{local}"))
+    import massively_b200 as mb
+    ex = mb.Executor(local)
+    wl = WORKLOADS[args.workload]()
+    wl.setup(ex)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = time_steps(ex, wl, args.steps, args.warmup, dist)
+    clocks = sampler.stop()
+    value = wl.value_from_ms(ms, world)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = wl.alg_bytes() / (ms * 1e-3) / 1e9
+    secondary = {}
+    if not args.no_secondary and args.workload == "sort_pairs_u32":
+        del wl.keys, wl.vals, wl.ko, wl.vo
+        for name in SECONDARY:
+            try:
+                w2 = WORKLOADS[name]()
+                w2.setup(ex)
+                ms2 = time_steps(ex, w2, max(3, args.steps), args.warmup, dist)
+                a2 = w2.alg_bytes() / (ms2 * 1e-3) / 1e9
+                secondary[name] = {"metric": w2.metric, "value": w2.value_from_ms(ms2, world),
+                                   "unit": w2.unit, "ms_per_step": ms2,
+                                   "roofline_frac": a2 / peak, "achieved_gbs": a2}
+                del w2
+                torch.cuda.empty_cache()
+            except Exception as e:  # a secondary that is not built yet
+                secondary[name] = {"error": str(e)[:200]}
+    e2e = None
+    if not args.no_e2e:
+        try:
+            torch.cuda.empty_cache()
+            e2e = e2e_measure(ex, WORKLOADS[args.workload](), max(1, min(args.steps, 3)))
+        except Exception as e:
+            e2e = {"error": str(e)[:200]}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(WORKLOADS[args.workload]())
+    if rank == 0:
+        line = {
+            "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": wl.dtype, "data": "synthetic (massively PCG streams, seeded)",
+            "config": {"workload": wl.name, "items_per_gpu": wl.n,
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": NCU_TRAFFIC_BYTES.get(wl.name),
+                         "kernel": wl.kernel,
+                         "note": "algorithmic bytes / CUDA-event time of the whole step"},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": gpu_launches(wl, args.steps),
+            "secondary": secondary or None,
+        }
+        print(json.dumps(line))
+    if dist:
+        import torch.distributed as D
+        D.destroy_process_group()
+
+
+def gpu_launches(wl, steps):
+    """Kernels this library launches per step, times steps."""
+    per = {"scan_kernel": 1, "select_kernel": 1, "radix_onesweep": 1 + 4}.get(wl.kernel, 1)
+    if isinstance(wl, SortPairsU32):
+        per = 1 + wl.passes
+    if isinstance(wl, SortU64):
+        per = 1 + 8
+    return per * steps
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]()
+    vals = []
+    t_all, u_all = 0.0, 0.0
+    for i in range(args.warmup + args.steps):
+        t, u = wl.cpu(wl.cpu_sample)
+        if i >= args.warmup:
+            vals.append(t)
+            t_all += t
+            u_all += u
+    v = u_all / t_all / 1e9
+    line = {
+        "impl": "reference", "metric": wl.metric, "value": v, "unit": wl.unit, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
+        "data": "synthetic (massively PCG streams, seeded)",
+        "config": {"workload": wl.name, "items_per_gpu": wl.n, "parallelism": "cpu",
+                   "sample_items_per_step": wl.cpu_sample},
+        "cpu_baseline": {"value": v, "unit": wl.unit, "cores": 1, "kind": "port",
+                         "sample": f"{wl.cpu_sample} items per step; the C++ restatement of "
+                                   "massively's sequential CPU oracle (its Rust oracle and "
+                                   "CubeCL runtimes do not build offline)"},
+        "e2e": {"value": v, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=os.environ.get("MB_BENCH_WORKLOAD", "sort_pairs_u32"),
+                    choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -185,9 +185,11 @@ uint64_t mb_executor_id(const mb_executor* exec);
  * device-side failure recorded since the last sync as MB_ERR_LAUNCH. */
 int mb_sync(mb_executor* exec);
 /* The stream the executor enqueues on (cudaStream_t, as void*).  Setting a
- * stream makes every later call enqueue there; NULL restores its own. */
+ * stream makes every later call enqueue there (NULL is the legacy default
+ * stream); mb_use_own_stream returns to the executor's own stream. */
 int mb_get_stream(mb_executor* exec, void** stream);
 int mb_set_stream(mb_executor* exec, void* stream);
+int mb_use_own_stream(mb_executor* exec);
 
 /* Executor::alloc / to_device / to_host (runtime.rs:98-177): stream-ordered
  * pool allocations owned by `exec`. */

@@ -1,0 +1,454 @@
+// radix.cu -- onesweep LSD radix sort (keys, or keys + one value column).
+//
+// Replaces massively's block-local 4-bit radix passes (massively/src/core/
+// radix.rs:120-546: per pass a block split of 256 items, a per-bucket
+// histogram prefix, a one-thread bucket-offset kernel and a scatter of a
+// permutation, then a final gather of the values; 8 passes for u32) with the
+// onesweep scheme:
+//
+//   1. histogram:  one read of the keys builds the 256-bin histograms of
+//                  every 8-bit digit at once;
+//   2. plan:       one block scans them into global digit offsets, marks
+//                  passes whose digit is the same for every key (skipped) and
+//                  assigns the ping-pong buffers so the last active pass lands
+//                  in the output -- on the device, so nothing synchronises and
+//                  the whole sort can be captured in a CUDA graph;
+//   3. onesweep:   per active digit, one kernel: every tile ranks its keys
+//                  stably (warp match on the digit, per-warp counters in
+//                  shared memory), publishes its 256 digit counts, obtains the
+//                  counts of all earlier tiles by a per-digit decoupled
+//                  look-back, and scatters keys (then values) through a
+//                  shared-memory staging buffer so consecutive threads write
+//                  consecutive addresses of each digit run.
+//
+// Keys are ordered by massively's radix encodings (massively/src/core/
+// radix.rs:46-89): unsigned as is, signed with the sign bit flipped, floats
+// in total order (negative: all bits inverted; otherwise sign bit set).  The
+// encoding only selects digits; keys move in their original bits.
+//
+// Byte model (8-bit digits): n*sk + 2*P*n*(sk+sv) for P digit passes.
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "lookback.cuh"
+
+namespace mb {
+namespace {
+
+constexpr int kRadixBits = 8;
+constexpr int kBins = 1 << kRadixBits;
+constexpr int kHistThreads = 256;
+constexpr uint32_t kCountMask = 0x3FFFFFFFu;  // status: 2 flag bits + 30 count bits
+
+template <class K>
+__device__ __forceinline__ uint32_t digit_of(K k, int shift) {
+  return (uint32_t)((radix_enc<K>(k) >> shift) & (kBins - 1));
+}
+
+// Buffer plan of one sort, filled on the device by the plan kernel.
+struct PassPlan {
+  const void* in_k[8];
+  void* out_k[8];
+  const void* in_v[8];
+  void* out_v[8];
+  uint32_t active[8];
+  uint32_t copy_only;
+  uint32_t pad_[3];
+};
+
+// ----------------------------------------------------------- histogram --
+
+template <class K, int PASSES>
+__global__ void __launch_bounds__(kHistThreads)
+    radix_histogram_kernel(const K* __restrict__ keys, uint64_t n, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t sh[PASSES][kBins];
+  for (int i = threadIdx.x; i < PASSES * kBins; i += kHistThreads) (&sh[0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t step = (uint64_t)gridDim.x * kHistThreads;
+  for (uint64_t i = blockIdx.x * (uint64_t)kHistThreads + threadIdx.x; i - threadIdx.x < n;
+       i += step) {
+    const bool valid = i < n;
+    const auto u = valid ? radix_enc<K>(keys[i]) : (typename UnsignedOf<K>::type)0;
+#pragma unroll
+    for (int p = 0; p < PASSES; ++p) {
+      const uint32_t d = (uint32_t)((u >> (p * kRadixBits)) & (kBins - 1));
+      // Whole warp on one digit (skewed keys): one add of the warp count.
+      const uint32_t d0 = __shfl_sync(kFull, d, 0);
+      const unsigned vmask = __ballot_sync(kFull, valid);
+      if (__all_sync(kFull, d == d0 || !valid)) {
+        if (lane_id() == 0 && vmask) atomicAdd(&sh[p][d0], (uint32_t)__popc(vmask));
+      } else if (valid) {
+        atomicAdd(&sh[p][d], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < PASSES * kBins; i += kHistThreads) {
+    uint32_t c = (&sh[0][0])[i];
+    if (c) atomicAdd(hist + i, c);
+  }
+}
+
+// ---------------------------------------------------------------- plan --
+
+// One block of 256 threads: exclusive digit offsets per pass (in place over
+// `hist`), trivial-pass detection and the buffer assignment.
+__global__ void __launch_bounds__(kBins)
+    radix_plan_kernel(uint32_t* __restrict__ hist, int passes, uint64_t n, PassPlan* plan,
+                      const void* in_k, void* out_k, void* tmp_k, const void* in_v, void* out_v,
+                      void* tmp_v) {
+  __shared__ uint32_t s_scan[kBins];
+  __shared__ uint32_t s_trivial[8];
+  const int d = threadIdx.x;
+  for (int p = 0; p < passes; ++p) {
+    const uint32_t c = hist[p * kBins + d];
+    if (d == 0) s_trivial[p] = 0;
+    __syncthreads();
+    if ((uint64_t)c == n) s_trivial[p] = 1;
+    s_scan[d] = c;
+    __syncthreads();
+    // Hillis-Steele inclusive scan over 256 bins.
+    for (int off = 1; off < kBins; off <<= 1) {
+      uint32_t v = d >= off ? s_scan[d - off] : 0;
+      __syncthreads();
+      s_scan[d] += v;
+      __syncthreads();
+    }
+    hist[p * kBins + d] = s_scan[d] - c;  // exclusive offset
+    __syncthreads();
+  }
+  if (d == 0) {
+    int m = 0;
+    for (int p = 0; p < passes; ++p) m += s_trivial[p] ? 0 : 1;
+    plan->copy_only = (m == 0 && n > 0) ? 1u : 0u;
+    int i = 0;  // index of the active pass among active passes
+    const void* cur_k = in_k;
+    const void* cur_v = in_v;
+    for (int p = 0; p < passes; ++p) {
+      if (s_trivial[p]) {
+        plan->active[p] = 0;
+        continue;
+      }
+      ++i;
+      // X_i is the output when (m - i) is even, else the temporary.
+      const bool to_out = ((m - i) % 2) == 0;
+      void* nk = to_out ? out_k : tmp_k;
+      void* nv = to_out ? out_v : tmp_v;
+      plan->active[p] = 1;
+      plan->in_k[p] = cur_k;
+      plan->out_k[p] = nk;
+      plan->in_v[p] = cur_v;
+      plan->out_v[p] = nv;
+      cur_k = nk;
+      cur_v = nv;
+    }
+    for (int p = passes; p < 8; ++p) plan->active[p] = 0;
+    if (plan->copy_only) {
+      plan->in_k[0] = in_k;
+      plan->out_k[0] = out_k;
+      plan->in_v[0] = in_v;
+      plan->out_v[0] = out_v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ onesweep --
+
+template <class K, class V, int THREADS, int ITEMS>
+struct OnesweepSmem {
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int TILE = THREADS * ITEMS;
+  uint32_t warp_cnt[WARPS][kBins];  // per-warp digit counts, then exclusive prefixes
+  uint32_t tile_start[kBins];       // exclusive prefix of the tile's digit counts
+  uint32_t delta[kBins];            // global base - tile start, per digit
+  uint32_t tile_id;
+  K keys[TILE];
+  V vals[std::is_same<V, uint8_t>::value ? 1 : TILE];
+};
+
+// V = uint8_t means "keys only".
+template <class K, class V, int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS)
+    radix_onesweep_kernel(const PassPlan* __restrict__ plan, int pass, uint64_t n,
+                          const uint32_t* __restrict__ digit_offsets, uint32_t* __restrict__ status,
+                          uint32_t* __restrict__ counter, uint32_t* __restrict__ err) {
+  constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
+  using S = OnesweepSmem<K, V, THREADS, ITEMS>;
+  constexpr int WARPS = S::WARPS;
+  constexpr int TILE = S::TILE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& sm = *reinterpret_cast<S*>(smem_raw);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+
+  if (plan->copy_only) {
+    // Every digit is constant: the stable order is the input order.
+    if (pass != 0) return;
+    const K* ik = (const K*)plan->in_k[0];
+    K* ok = (K*)plan->out_k[0];
+    const V* iv = (const V*)plan->in_v[0];
+    V* ov = (V*)plan->out_v[0];
+    for (uint64_t i = blockIdx.x * (uint64_t)THREADS + tid; i < n;
+         i += (uint64_t)gridDim.x * THREADS) {
+      if (ok) ok[i] = ik[i];
+      if constexpr (!KEYS_ONLY) ov[i] = iv[i];
+    }
+    return;
+  }
+  if (!plan->active[pass]) return;
+  const K* __restrict__ in_k = (const K*)plan->in_k[pass];
+  K* __restrict__ out_k = (K*)plan->out_k[pass];
+  const V* __restrict__ in_v = (const V*)plan->in_v[pass];
+  V* __restrict__ out_v = (V*)plan->out_v[pass];
+  const int shift = pass * kRadixBits;
+
+  if (tid == 0) sm.tile_id = atomicAdd(counter, 1u);
+  for (int i = tid; i < WARPS * kBins; i += THREADS) (&sm.warp_cnt[0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t tile = sm.tile_id;
+  const uint64_t tile_base = tile * (uint64_t)TILE;
+  const uint64_t warp_base = tile_base + (uint64_t)warp * 32 * ITEMS;
+
+  // Warp-striped loads: item k of lane l is at warp_base + k*32 + l, so the
+  // rounds below visit the keys in input order (stability).
+  K key[ITEMS];
+  uint32_t dig[ITEMS];
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+    if (i < n) {
+      key[k] = __ldcs(in_k + i);
+      dig[k] = digit_of<K>(key[k], shift);
+    } else {
+      key[k] = K(0);
+      dig[k] = kBins;  // out-of-range digit: never counted or written
+    }
+  }
+  V val[KEYS_ONLY ? 1 : ITEMS];
+  if constexpr (!KEYS_ONLY) {
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+      val[k] = i < n ? __ldcs(in_v + i) : V(0);
+    }
+  }
+
+  // Stable rank within the warp: peers with the same digit in a round are
+  // ordered by lane; rounds are in input order.
+  uint32_t rank[ITEMS];
+  const unsigned lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t d = dig[k];
+    const unsigned peers = __match_any_sync(kFull, d);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader && d < kBins) {
+      base = sm.warp_cnt[warp][d];
+      sm.warp_cnt[warp][d] = base + __popc(peers);
+    }
+    base = __shfl_sync(kFull, base, leader);
+    rank[k] = base + __popc(peers & lt_mask);
+    __syncwarp();  // order this round's counter update before the next round's read
+  }
+  __syncthreads();
+
+  // Per digit (thread d): exclusive prefix over warps, tile count.
+  uint32_t tile_count = 0;
+  if (tid < kBins) {
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+      const uint32_t c = sm.warp_cnt[w][tid];
+      sm.warp_cnt[w][tid] = tile_count;
+      tile_count += c;
+    }
+    // Publish this tile's count for digit `tid`.
+    uint32_t* row = status + tile * kBins;
+    const uint32_t flag = tile == 0 ? kFlagIncl : kFlagAgg;
+    st_relaxed_u32(row + tid, (flag << 30) | tile_count);
+  }
+  // Tile-local exclusive scan of the digit counts (block scan over 256).
+  if (tid < kBins) sm.tile_start[tid] = tile_count;
+  __syncthreads();
+  for (int off = 1; off < kBins; off <<= 1) {
+    uint32_t v = 0;
+    if (tid < kBins && tid >= off) v = sm.tile_start[tid - off];
+    __syncthreads();
+    if (tid < kBins) sm.tile_start[tid] += v;
+    __syncthreads();
+  }
+  if (tid < kBins) sm.tile_start[tid] -= tile_count;
+
+  // Decoupled look-back, one digit per thread.
+  if (tid < kBins) {
+    uint32_t excl = 0;
+    if (tile > 0) {
+      SpinGuard guard(err);
+      int64_t t = (int64_t)tile - 1;
+      bool failed = false;
+      while (t >= 0) {
+        const uint32_t w = ld_relaxed_u32(status + (uint64_t)t * kBins + tid);
+        const uint32_t f = w >> 30;
+        if (f == kFlagNone) {
+          if (guard.expired()) { failed = true; break; }
+          continue;
+        }
+        excl += w & kCountMask;
+        if (f == kFlagIncl) break;
+        --t;
+      }
+      if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+      st_relaxed_u32(status + tile * kBins + tid, (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
+    }
+    sm.delta[tid] = digit_offsets[pass * kBins + tid] + excl - sm.tile_start[tid];
+  }
+  __syncthreads();
+
+  // Stage keys in shared memory in tile-sorted order.
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t d = dig[k];
+    if (d < kBins) {
+      const uint32_t pos = sm.tile_start[d] + sm.warp_cnt[warp][d] + rank[k];
+      rank[k] = pos;
+      sm.keys[pos] = key[k];
+      if constexpr (!KEYS_ONLY) sm.vals[pos] = val[k];
+    }
+  }
+  __syncthreads();
+  const uint64_t valid = n - tile_base < (uint64_t)TILE ? n - tile_base : (uint64_t)TILE;
+  // Coalesced write-out: position i of the sorted tile goes to delta[d] + i.
+#pragma unroll 4
+  for (int i = tid; i < (int)valid; i += THREADS) {
+    const K kk = sm.keys[i];
+    const uint32_t d = digit_of<K>(kk, shift);
+    const uint32_t o = sm.delta[d] + (uint32_t)i;
+    if (o >= n) {  // only reachable after a failed look-back
+      raise_device_error(err, MB_DEV_ERR_BOUNDS);
+      continue;
+    }
+    __stcs(out_k + o, kk);
+    if constexpr (!KEYS_ONLY) __stcs(out_v + o, sm.vals[i]);
+  }
+}
+
+template <class K, class V, int THREADS, int ITEMS>
+size_t onesweep_smem() {
+  return sizeof(OnesweepSmem<K, V, THREADS, ITEMS>);
+}
+
+// Tile configurations of the onesweep kernel (MB_TUNE_RADIX).
+struct RadixCfg {
+  int threads, items;
+  const char* text;
+};
+constexpr RadixCfg kRadixCfgs[] = {
+    {256, 16, "onesweep 256 threads x 16 keys (4096-key tiles)"},
+    {256, 24, "onesweep 256 threads x 24 keys (6144-key tiles)"},
+    {512, 16, "onesweep 512 threads x 16 keys (8192-key tiles)"},
+};
+constexpr int kRadixDefault = 0;
+
+template <class K, class V, int THREADS, int ITEMS>
+int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v,
+                      uint64_t n) {
+  constexpr int PASSES = (int)sizeof(K);
+  constexpr int TILE = THREADS * ITEMS;
+  constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
+  const uint64_t tiles = (n + TILE - 1) / TILE;
+  if (n >= (1ull << 30))
+    return set_error(MB_ERR_LENGTH_TOO_LARGE, "radix sort supports fewer than 2^30 items", n);
+  // Scratch: [plan][hist P*256][counters P (padded)][status P*tiles*256]
+  // [tmp keys][tmp values]
+  const size_t plan_b = ((sizeof(PassPlan) + 255) / 256) * 256;
+  const size_t hist_b = (size_t)PASSES * kBins * 4;
+  const size_t cnt_b = 256;
+  const size_t status_b = (size_t)PASSES * tiles * kBins * 4;
+  const size_t zero_b = plan_b + hist_b + cnt_b + status_b;
+  const size_t tk_b = ((n * sizeof(K) + 255) / 256) * 256;
+  const size_t tv_b = KEYS_ONLY ? 0 : ((n * sizeof(V) + 255) / 256) * 256;
+  Scratch scratch;
+  MB_TRY(scratch.alloc(ex, zero_b + tk_b + tv_b + (out_k ? 0 : tk_b)));
+  char* base = scratch.as<char>();
+  PassPlan* plan = (PassPlan*)base;
+  uint32_t* hist = (uint32_t*)(base + plan_b);
+  uint32_t* counters = (uint32_t*)(base + plan_b + hist_b);
+  uint32_t* status = (uint32_t*)(base + plan_b + hist_b + cnt_b);
+  K* tmp_k = (K*)(base + zero_b);
+  V* tmp_v = KEYS_ONLY ? nullptr : (V*)(base + zero_b + tk_b);
+  K* final_k = out_k ? out_k : (K*)(base + zero_b + tk_b + tv_b);
+  MB_CUDA(cudaMemsetAsync(base, 0, zero_b, ex->stream));
+
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ex->device);
+  const uint64_t hist_blocks = std::min<uint64_t>((n + kHistThreads * 16 - 1) / (kHistThreads * 16),
+                                                  (uint64_t)sms * 4);
+  radix_histogram_kernel<K, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks), kHistThreads,
+                                      0, ex->stream>>>(in_k, n, hist);
+  MB_CUDA(cudaGetLastError());
+  radix_plan_kernel<<<1, kBins, 0, ex->stream>>>(hist, PASSES, n, plan, in_k, final_k, tmp_k,
+                                                 in_v, out_v, tmp_v);
+  MB_CUDA(cudaGetLastError());
+  const size_t smem = onesweep_smem<K, V, THREADS, ITEMS>();
+  auto kern = radix_onesweep_kernel<K, V, THREADS, ITEMS>;
+  MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int p = 0; p < PASSES; ++p) {
+    kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(plan, p, n, hist, status + (size_t)p * tiles * kBins,
+                                                         counters + p, ex->status_dev);
+    MB_CUDA(cudaGetLastError());
+  }
+  return MB_OK;
+}
+
+template <class K, class V>
+int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v, uint64_t n) {
+  if (n == 0) return MB_OK;
+  int cfg = ex->tune[MB_TUNE_RADIX];
+  if (cfg < 0) cfg = kRadixDefault;
+  switch (cfg) {
+    case 1: return onesweep_sort_cfg<K, V, 256, 24>(ex, in_k, in_v, out_k, out_v, n);
+    case 2: return onesweep_sort_cfg<K, V, 512, 16>(ex, in_k, in_v, out_k, out_v, n);
+    default: return onesweep_sort_cfg<K, V, 256, 16>(ex, in_k, in_v, out_k, out_v, n);
+  }
+}
+
+// Dispatch on the key type and the value width (0 = keys only, 4, 8).
+template <class K>
+int sort_keys_vals(mb_executor* ex, const void* ik, const void* iv, void* ok, void* ov,
+                   size_t vsize, uint64_t n) {
+  switch (vsize) {
+    case 0: return onesweep_sort<K, uint8_t>(ex, (const K*)ik, nullptr, (K*)ok, nullptr, n);
+    case 4: return onesweep_sort<K, uint32_t>(ex, (const K*)ik, (const uint32_t*)iv, (K*)ok,
+                                              (uint32_t*)ov, n);
+    case 8: return onesweep_sort<K, uint64_t>(ex, (const K*)ik, (const uint64_t*)iv, (K*)ok,
+                                              (uint64_t*)ov, n);
+    default: return set_error(MB_ERR_LAUNCH, "radix values must be 4 or 8 bytes wide");
+  }
+}
+
+}  // namespace
+
+// Radix sort of plain device columns: keys of type `kdt` (32- or 64-bit
+// elements), values of `vsize` bytes (0 = none).  out_k may be null.
+int radix_sort_plain(mb_executor* ex, int kdt, const void* ik, const void* iv, void* ok, void* ov,
+                     size_t vsize, uint64_t n) {
+  switch (kdt) {
+    case MB_U32: return sort_keys_vals<uint32_t>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_I32: return sort_keys_vals<int32_t>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_F32: return sort_keys_vals<float>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_U64: return sort_keys_vals<uint64_t>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_I64: return sort_keys_vals<int64_t>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_F64: return sort_keys_vals<double>(ex, ik, iv, ok, ov, vsize, n);
+    default: return set_error(MB_ERR_LAUNCH, "radix keys must be 32- or 64-bit elements");
+  }
+}
+
+int radix_tune_count() { return (int)(sizeof(kRadixCfgs) / sizeof(kRadixCfgs[0])); }
+const char* radix_tune_text(int c) {
+  return (c >= 0 && c < radix_tune_count()) ? kRadixCfgs[c].text : nullptr;
+}
+
+}  // namespace mb

@@ -1,0 +1,264 @@
+// select.cu -- stable compaction: vector::copy_where, remove_where and
+// partition in one pass over the data.
+//
+// Replaces massively's selection control (massively/src/core/selection.rs:
+// 149-457: a three-kernel scan of the flags into positions, a kernel turning
+// positions into compacted source indices, then a gather -- about five
+// passes) with one kernel per call: each tile evaluates its flags (the
+// stencil view, or a predicate fused onto the column being compacted so the
+// column is read once), ranks kept rows with warp ballots (warp-striped
+// items, so ranks follow input order), gets the kept-row count of all
+// earlier tiles by decoupled look-back and writes every column's kept rows
+// to consecutive output positions.  The count of kept rows stays on the
+// device (massively's LogicalExtent::Device, massively/src/core/
+// extent.rs:17-36).  partition writes rejected rows after the kept ones,
+// both stable; its boundary comes from one reduction of the flags first.
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "lookback.cuh"
+
+namespace mb {
+
+int materialize(mb_executor* ex, const mb_src& in, void* dst);
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;
+constexpr int kMaxCols = 12;
+
+enum SelMode : int { kCopy = 0, kRemove = 1, kPartition = 2 };
+
+struct SelParams {
+  int ncols;
+  int mode;
+  int fused;                  // stencil = predicate `fused_map` over column 0's data
+  int fused_map;
+  Src cols[kMaxCols];
+  void* outs[kMaxCols];
+  int esize[kMaxCols];
+  Src stencil;
+  uint32_t* count_dev;
+  const uint32_t* boundary_dev;  // partition: number of kept rows
+  uint32_t* counter;
+  uint32_t* status;
+};
+
+__device__ __forceinline__ void st_raw(void* p, uint64_t i, int esize, uint64_t bits) {
+  switch (esize) {
+    case 1: ((uint8_t*)p)[i] = (uint8_t)bits; break;
+    case 2: ((uint16_t*)p)[i] = (uint16_t)bits; break;
+    case 4: ((uint32_t*)p)[i] = (uint32_t)bits; break;
+    default: ((uint64_t*)p)[i] = bits; break;
+  }
+}
+
+// FAST: one plain 4-byte column, flags fused on it or a plain u32 stencil.
+template <bool FAST>
+__global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t cap,
+                                                          TileState<uint32_t, true> st) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_wcount[kWarps];
+  __shared__ uint32_t s_excl;
+  if (threadIdx.x == 0) s_tile = atomicAdd(p.counter, 1u);
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t n = src_len(p.cols[0]) < cap ? src_len(p.cols[0]) : cap;
+  const uint64_t tile_base = tile * (uint64_t)kTile;
+  if (tile_base >= n) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t warp_base = tile_base + (uint64_t)warp * 32 * kItems;
+  const uint32_t invert = p.mode == kRemove ? 1u : 0u;
+
+  uint32_t v0[FAST ? kItems : 1];
+  unsigned ballot[kItems];
+  uint32_t wcount = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+    const bool valid = i < n;
+    uint32_t f = 0;
+    if (valid) {
+      if constexpr (FAST) {
+        v0[k] = __ldcs((const uint32_t*)p.cols[0].data + i);
+        if (p.fused) f = map_to<uint32_t>(p.fused_map, p.cols[0].dtype, v0[k]) != 0;
+        else f = __ldcs((const uint32_t*)p.stencil.data + i) != 0;
+      } else {
+        f = src_load<uint32_t>(p.stencil, i) != 0;
+      }
+      f ^= invert;
+    }
+    ballot[k] = __ballot_sync(kFull, valid && f);
+    wcount += __popc(ballot[k]);
+  }
+  if (lane == 0) s_wcount[warp] = wcount;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t c = lane < kWarps ? s_wcount[lane] : 0u;
+    uint32_t agg = __reduce_add_sync(kFull, c);
+    const Op<uint32_t, MB_OP_ADD> add{MB_OP_ADD};
+    uint32_t excl = 0;
+    if (tile == 0) {
+      if (lane == 0) st.publish(0, kFlagIncl, agg);
+    } else {
+      if (lane == 0) st.publish(tile, kFlagAgg, agg);
+      excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add,
+                                                                           p.status, 0u);
+      if (lane == 0) st.publish(tile, kFlagIncl, excl + agg);
+    }
+    if (lane == 0) {
+      s_excl = excl;
+      if (tile_base + kTile >= n && p.count_dev) *p.count_dev = excl + agg;
+    }
+  }
+  __syncthreads();
+  uint32_t before = s_excl;  // kept rows before this warp's chunk
+  for (int w = 0; w < warp; ++w) before += s_wcount[w];
+  const unsigned lt = (1u << lane) - 1u;
+  const uint64_t boundary = p.mode == kPartition ? *p.boundary_dev : 0;
+
+  // Per item: output position (or ~0 when the row is not written).
+  uint32_t pos[kItems];
+  uint32_t run = before;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+    const bool kept = (ballot[k] >> lane) & 1u;
+    const uint32_t r = run + __popc(ballot[k] & lt);
+    if (kept) pos[k] = r;
+    else if (p.mode == kPartition && i < n) pos[k] = (uint32_t)(boundary + i - r);
+    else pos[k] = 0xFFFFFFFFu;
+    run += __popc(ballot[k]);
+  }
+  if constexpr (FAST) {
+    uint32_t* out = (uint32_t*)p.outs[0];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k)
+      if (pos[k] != 0xFFFFFFFFu) out[pos[k]] = v0[k];
+  } else {
+    for (int c = 0; c < p.ncols; ++c) {
+#pragma unroll 4
+      for (int k = 0; k < kItems; ++k) {
+        if (pos[k] == 0xFFFFFFFFu) continue;
+        const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+        st_raw(p.outs[c], pos[k], p.esize[c], src_load_bits(p.cols[c], i));
+      }
+    }
+  }
+}
+
+int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* stencil,
+                 const mb_col* out, uint32_t* count_dev, uint32_t* count_host, int mode,
+                 uint32_t* boundary_dev) {
+  MB_TRY(check_exec(ex));
+  if (ncols < 1 || ncols > kMaxCols) return set_error(MB_ERR_LAUNCH, "1 to 12 columns");
+  if (!in || !out) return set_error(MB_ERR_UNBOUND_COLUMN, "missing columns");
+  const uint64_t n = in[0].len;
+  for (int c = 0; c < ncols; ++c) {
+    MB_TRY(check_src(ex, &in[c], "input"));
+    MB_TRY(check_col(ex, out[c], "output"));
+    if (in[c].len != n) return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", n, in[c].len);
+    if (out[c].len < n)
+      return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", n, out[c].len);
+    if (dtype_size(out[c].dtype) != dtype_size(in[c].vtype))
+      return set_error(MB_ERR_LAUNCH, "output element type differs from the input's");
+  }
+  MB_TRY(check_src(ex, stencil, "stencil"));
+  if (stencil->len != n)
+    return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", n, stencil->len);
+  Scratch cnt_tmp;
+  if (!count_dev) {
+    MB_TRY(cnt_tmp.alloc(ex, 16));
+    count_dev = cnt_tmp.as<uint32_t>();
+  }
+  if (n == 0) {
+    MB_CUDA(cudaMemsetAsync(count_dev, 0, 4, ex->stream));
+  } else {
+    SelParams p{};
+    p.ncols = ncols;
+    p.mode = mode;
+    for (int c = 0; c < ncols; ++c) {
+      p.cols[c] = to_src(in[c]);
+      p.outs[c] = out[c].data;
+      p.esize[c] = (int)dtype_size(in[c].vtype);
+    }
+    p.stencil = to_src(*stencil);
+    p.count_dev = count_dev;
+    p.boundary_dev = boundary_dev;
+    // The predicate reads the same elements as column 0: evaluate it on the
+    // loaded values (the column is read once).
+    const bool same_data = stencil->kind == MB_SRC_COLUMN && in[0].kind == MB_SRC_COLUMN &&
+                           stencil->data == in[0].data && stencil->dtype == in[0].dtype &&
+                           in[0].map == MB_UN_IDENTITY;
+    p.fused = same_data && stencil->map != MB_UN_IDENTITY;
+    p.fused_map = stencil->map;
+    const bool fast = ncols == 1 && src_plain(in[0], in[0].vtype) &&
+                      dtype_size(in[0].vtype) == 4 && in[0].len_dev == nullptr &&
+                      (p.fused || (src_plain(*stencil, MB_U32) && stencil->vtype == MB_U32 &&
+                                   stencil->dtype == MB_U32 && stencil->len_dev == nullptr));
+    const uint64_t tiles = (n + kTile - 1) / kTile;
+    Scratch scratch;
+    MB_TRY(scratch.alloc(ex, 256 + tiles * 8));
+    MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + tiles * 8, ex->stream));
+    p.counter = scratch.as<uint32_t>();
+    p.status = ex->status_dev;
+    auto st = TileState<uint32_t, true>::make(scratch.as<char>() + 256, tiles);
+    if (fast)
+      select_kernel<true><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    else
+      select_kernel<false><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    MB_CUDA(cudaGetLastError());
+  }
+  if (count_host) MB_TRY(read_u32(ex, count_dev, count_host));
+  return MB_OK;
+}
+
+}  // namespace
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" {
+
+int mb_copy_where(mb_executor* ex, const mb_src* in, int ncols, const mb_src* stencil,
+                  const mb_col* out, uint32_t* count_dev, uint32_t* count_host) {
+  return select_entry(ex, in, ncols, stencil, out, count_dev, count_host, kCopy, nullptr);
+}
+
+int mb_remove_where(mb_executor* ex, const mb_src* in, int ncols, const mb_src* stencil,
+                    const mb_col* out, uint32_t* count_dev, uint32_t* count_host) {
+  return select_entry(ex, in, ncols, stencil, out, count_dev, count_host, kRemove, nullptr);
+}
+
+int mb_partition(mb_executor* ex, const mb_src* in, int ncols, int pred_col, int pred,
+                 const mb_col* out, uint32_t* boundary_dev, uint32_t* boundary_host) {
+  MB_TRY(check_exec(ex));
+  if (!in || ncols < 1 || ncols > 12 || pred_col < 0 || pred_col >= ncols)
+    return set_error(MB_ERR_LAUNCH, "partition: bad column selection");
+  if (pred < MB_UN_IS_TRUE || pred > MB_UN_IS_POSITIVE || pred == MB_UN_NEGATE ||
+      pred == MB_UN_BIT_NOT || pred == MB_UN_ABS)
+    return set_error(MB_ERR_LAUNCH, "partition needs a predicate");
+  // The stencil: the predicate over column pred_col, as a view.
+  mb_src stencil = in[pred_col];
+  if (stencil.map != MB_UN_IDENTITY || stencil.dtype != stencil.vtype) {
+    return set_error(MB_ERR_LAUNCH, "partition predicate column must not be a mapped view");
+  }
+  stencil.map = pred;
+  stencil.vtype = MB_U32;
+  Scratch bnd;
+  if (!boundary_dev) {
+    MB_TRY(bnd.alloc(ex, 16));
+    boundary_dev = bnd.as<uint32_t>();
+  }
+  const uint32_t zero = 0;
+  MB_TRY(mb_reduce(ex, &stencil, MB_OP_ADD, &zero, boundary_dev, nullptr));
+  MB_TRY(select_entry(ex, in, ncols, &stencil, out, nullptr, nullptr, kPartition, boundary_dev));
+  if (boundary_host) MB_TRY(read_u32(ex, boundary_dev, boundary_host));
+  return MB_OK;
+}
+
+}  // extern "C"

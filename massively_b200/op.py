@@ -1,0 +1,74 @@
+"""Built-in operators: the compile-time `op::*` traits of massively, as ids.
+
+massively lets users write `#[cube]` operators (ReductionOp, UnaryOp,
+PredicateOp, BinaryPredicateOp: massively/src/core/op.rs:33-96,
+massively/src/core/reduce.rs:63-66, massively/src/core/ordering/mod.rs:53-56);
+this library compiles a fixed set of them into its kernels
+(include/massively_b200.h mb_op / mb_unary / mb_pred2).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+
+@dataclass(frozen=True)
+class ReductionOp:
+    id: int
+    name: str
+    commutative: bool = True
+
+
+@dataclass(frozen=True)
+class UnaryOp:
+    id: int
+    name: str
+    is_predicate: bool = False
+
+
+@dataclass(frozen=True)
+class BinaryPredicateOp:
+    id: int
+    name: str
+
+
+Add = ReductionOp(0, "add")
+Mul = ReductionOp(1, "mul")
+Min = ReductionOp(2, "min")
+Max = ReductionOp(3, "max")
+BitAnd = ReductionOp(4, "and")
+BitOr = ReductionOp(5, "or")
+BitXor = ReductionOp(6, "xor")
+TakeLeft = ReductionOp(7, "take_left", commutative=False)
+TakeRight = ReductionOp(8, "take_right", commutative=False)
+REDUCTIONS = {o.name: o for o in (Add, Mul, Min, Max, BitAnd, BitOr, BitXor, TakeLeft, TakeRight)}
+
+Identity = UnaryOp(0, "identity")
+IsTrue = UnaryOp(1, "is_true", True)
+IsFalse = UnaryOp(2, "is_false", True)
+IsEven = UnaryOp(3, "is_even", True)
+IsOdd = UnaryOp(4, "is_odd", True)
+Negate = UnaryOp(5, "negate")
+BitNot = UnaryOp(6, "bit_not")
+Abs = UnaryOp(7, "abs")
+IsNegative = UnaryOp(8, "is_negative", True)
+IsPositive = UnaryOp(9, "is_positive", True)
+UNARIES = {o.name: o for o in (Identity, IsTrue, IsFalse, IsEven, IsOdd, Negate, BitNot, Abs,
+                               IsNegative, IsPositive)}
+
+Less = BinaryPredicateOp(0, "less")
+Greater = BinaryPredicateOp(1, "greater")
+TotalLess = BinaryPredicateOp(2, "total_less")
+Equal = BinaryPredicateOp(3, "equal")
+PREDICATES2 = {o.name: o for o in (Less, Greater, TotalLess, Equal)}
+
+
+def reduction(op) -> ReductionOp:
+    return REDUCTIONS[op] if isinstance(op, str) else op
+
+
+def unary(op) -> UnaryOp:
+    return UNARIES[op] if isinstance(op, str) else op
+
+
+def pred2(op) -> BinaryPredicateOp:
+    return PREDICATES2[op] if isinstance(op, str) else op

@@ -1,0 +1,203 @@
+"""`seg::*`: Segmentation and per-segment algorithms over the C ABI.
+
+Mirrors massively/src/seg/segmentation.rs:129-441 (Segmentation: offsets are
+canonical, validated with one synchronisation) and massively/src/seg/
+mod.rs:159-243 (ForEachSegment(algorithm).run(exec, segments)).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from . import op as O
+from .lazy import lower
+from .runtime import (DeviceVec, Executor, ForeignExecutor, InvalidSegmentation, LengthMismatch,
+                      LengthTooLarge, MINDEX_MAX, check, scalar_buffer)
+
+_L = N.lib
+U32 = np.dtype(np.uint32)
+
+
+class Segmentation:
+    """A validated partition of a flat value range into ordered segments."""
+
+    def __init__(self, offsets: DeviceVec, value_count: int):
+        self._offsets = offsets
+        self._value_count = int(value_count)
+
+    @classmethod
+    def from_offsets(cls, exec: Executor, offsets) -> "Segmentation":
+        """Segmentation::from_offsets (segmentation.rs:196-232)."""
+        off = _u32_column(exec, offsets)
+        if len(off) == 0:
+            raise InvalidSegmentation()
+        vc = C.c_uint32(0)
+        check(_L().mb_segmentation_validate_offsets(exec.handle, C.c_void_p(off.data_ptr()),
+                                                    len(off), C.byref(vc)))
+        return cls(off, vc.value)
+
+    @classmethod
+    def from_lengths(cls, exec: Executor, lengths) -> "Segmentation":
+        """Segmentation::from_lengths (segmentation.rs:238-280)."""
+        n = len(lengths)
+        if n >= MINDEX_MAX:
+            raise LengthTooLarge(n + 1)
+        keep = []
+        s = lower(exec, lengths, keep) if n else None
+        off = exec.alloc(U32, n + 1)
+        if n == 0:
+            off.tensor.zero_()
+            return cls(off, 0)
+        vc = C.c_uint32(0)
+        check(_L().mb_segmentation_from_lengths(exec.handle, C.byref(s),
+                                                C.c_void_p(off.data_ptr()), C.byref(vc)))
+        return cls(off, vc.value)
+
+    @classmethod
+    def from_segment_ids(cls, exec: Executor, ids, segment_count: int) -> "Segmentation":
+        """Segmentation::from_segment_ids (segmentation.rs:290-335): ids must be
+        non-decreasing and < segment_count."""
+        if segment_count >= MINDEX_MAX:
+            raise LengthTooLarge(segment_count + 1)
+        idv = _u32_column(exec, ids)
+        t = idv.tensor
+        if len(idv):
+            bad = (t[-1:].to(__import__("torch").int64) >= segment_count).any()
+            if len(idv) > 1:
+                bad = bad | (t[1:].to(__import__("torch").int64) <
+                             t[:-1].to(__import__("torch").int64)).any()
+            if bool(bad):
+                raise InvalidSegmentation()
+        import torch
+        counts = torch.bincount(t.to(torch.int64), minlength=segment_count) if len(idv) else \
+            torch.zeros(segment_count, dtype=torch.int64, device=t.device)
+        off = torch.zeros(segment_count + 1, dtype=torch.int64, device=t.device)
+        off[1:] = torch.cumsum(counts, 0)
+        return cls(exec.from_tensor(off.to(torch.uint32)), len(idv))
+
+    def offsets(self) -> DeviceVec:
+        return self._offsets
+
+    def segment_count(self) -> int:
+        return len(self._offsets) - 1
+
+    def value_count(self) -> int:
+        return self._value_count
+
+    def lengths(self, exec: Executor) -> DeviceVec:
+        t = self._offsets.tensor
+        import torch
+        d = (t[1:].to(torch.int64) - t[:-1].to(torch.int64)).to(torch.uint32)
+        return exec.from_tensor(d.contiguous())
+
+    def segment_ids(self, exec: Executor) -> DeviceVec:
+        """Segmentation::segment_ids: flat value -> segment index."""
+        out = exec.alloc(U32, self._value_count)
+        if self._value_count:
+            check(_L().mb_segmentation_segment_ids(
+                exec.handle, C.c_void_p(self._offsets.data_ptr()), self.segment_count(),
+                C.c_void_p(out.data_ptr()), self._value_count))
+        return out
+
+    def local_indices(self, exec: Executor) -> DeviceVec:
+        ids = self.segment_ids(exec)
+        import torch
+        pos = torch.arange(self._value_count, device=ids.tensor.device, dtype=torch.int64)
+        starts = self._offsets.tensor.to(torch.int64)[ids.tensor.to(torch.int64)]
+        return exec.from_tensor((pos - starts).to(torch.uint32))
+
+    def segments(self, values) -> "SegmentIterator":
+        if len(values) != self._value_count:
+            raise LengthMismatch(self._value_count, len(values))
+        return SegmentIterator(values, self)
+
+
+class SegmentIterator:
+    """Values paired with their segmentation (seg/mod.rs:49-99)."""
+
+    def __init__(self, values, segmentation: Segmentation):
+        self._values, self._seg = values, segmentation
+
+    def values(self):
+        return self._values
+
+    def offsets(self) -> DeviceVec:
+        return self._seg.offsets()
+
+    def segmentation(self) -> Segmentation:
+        return self._seg
+
+
+def _u32_column(exec: Executor, x) -> DeviceVec:
+    from .lazy import _as_column
+    keep = []
+    col = _as_column(exec, x, keep)
+    if col.dtype != U32:
+        raise LengthMismatch(4, col.dtype.itemsize)
+    if col.owner != exec.id:
+        raise ForeignExecutor()
+    return col
+
+
+# --------------------------------------------------------- algorithms ------
+
+class InclusiveScan:
+    def __init__(self, op):
+        self.op = O.reduction(op)
+
+
+class ExclusiveScan:
+    def __init__(self, op, init):
+        self.op, self.init = O.reduction(op), init
+
+
+class Reduce:
+    def __init__(self, op, init):
+        self.op, self.init = O.reduction(op), init
+
+
+class Sort:
+    def __init__(self, less=O.Less):
+        self.less = O.pred2(less)
+
+
+class ForEachSegment:
+    """ForEachSegment(algorithm).run(exec, segments) (seg/mod.rs:159-243).
+    Scans and sorts return a SegmentIterator over new values with the same
+    offsets; Reduce returns one value per segment (empty -> init)."""
+
+    def __init__(self, algorithm):
+        self.algorithm = algorithm
+
+    def run(self, exec: Executor, segments: SegmentIterator):
+        a = self.algorithm
+        values, sgm = segments.values(), segments.segmentation()
+        keep = []
+        s = lower(exec, values, keep)
+        off = C.c_void_p(sgm.offsets().data_ptr())
+        nseg = sgm.segment_count()
+        dt = values.dtype
+        if isinstance(a, InclusiveScan):
+            out = exec.alloc(dt, len(values))
+            check(_L().mb_seg_inclusive_scan(exec.handle, C.byref(s), off, nseg, a.op.id,
+                                             out.to_col()))
+            return SegmentIterator(out, sgm)
+        if isinstance(a, ExclusiveScan):
+            out = exec.alloc(dt, len(values))
+            buf = scalar_buffer(a.init, dt)
+            check(_L().mb_seg_exclusive_scan(exec.handle, C.byref(s), off, nseg, a.op.id, buf,
+                                             out.to_col()))
+            return SegmentIterator(out, sgm)
+        if isinstance(a, Reduce):
+            out = exec.alloc(dt, nseg)
+            buf = scalar_buffer(a.init, dt)
+            check(_L().mb_seg_reduce(exec.handle, C.byref(s), off, nseg, a.op.id, buf,
+                                     out.to_col()))
+            return out
+        if isinstance(a, Sort):
+            out = exec.alloc(dt, len(values))
+            check(_L().mb_seg_sort(exec.handle, C.byref(s), off, nseg, a.less.id, out.to_col()))
+            return SegmentIterator(out, sgm)
+        raise TypeError(f"unsupported segment algorithm {type(a).__name__}")

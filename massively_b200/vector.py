@@ -1,0 +1,522 @@
+"""`vector::*` algorithms of massively over the C ABI.
+
+Each function mirrors the public function of massively/src/api/algorithm/
+named in its docstring (same argument order and meaning, same errors) and
+runs on the executor's stream through libmassively_b200.so.  Inputs may be
+DeviceVecs, lazy views (massively_b200.lazy) or zips of them; outputs are
+new DeviceVecs (zips for multi-column rows).  Length-changing results carry
+their count on the device (DeviceVec.len_dev), as massively's
+LogicalExtent::Device does, so pipelines need no host synchronisation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import op as O
+from .iter import Zip
+from .lazy import View, lower
+from .runtime import (ID_TO_NP, DeviceVec, Executor, ForeignExecutor, LengthMismatch,
+                      LengthTooLarge, MINDEX_MAX, check, scalar_buffer)
+
+_L = N.lib
+
+
+def _columns(x) -> list:
+    return list(x.cols) if isinstance(x, Zip) else [x]
+
+
+def _srcs(exec: Executor, x, keep: list):
+    cols = _columns(x)
+    arr = (N.mb_src * len(cols))()
+    for k, c in enumerate(cols):
+        arr[k] = lower(exec, c, keep)
+    return arr, len(cols)
+
+
+def _out_like(exec: Executor, x, n: int, len_dev=None):
+    outs = []
+    for c in _columns(x):
+        v = exec.alloc(c.dtype, n)
+        if len_dev is not None:
+            v = v.with_len_dev(len_dev)
+        outs.append(v)
+    return outs
+
+
+def _cols(outs) -> C.Array:
+    arr = (N.mb_col * len(outs))()
+    for k, o in enumerate(outs):
+        arr[k] = o.to_col()
+    return arr
+
+
+def _wrap(x, outs):
+    return Zip(*outs) if isinstance(x, Zip) else outs[0]
+
+
+def _check_owner(exec: Executor, *xs):
+    for x in xs:
+        for c in _columns(x):
+            if isinstance(c, DeviceVec) and c.owner != exec.id:
+                raise ForeignExecutor()
+
+
+def _len(x) -> int:
+    n = len(x)
+    if n > MINDEX_MAX:
+        raise LengthTooLarge(n)
+    return n
+
+
+def _dtype(x):
+    return _columns(x)[0].dtype
+
+
+def _len_dev_of(x):
+    c = _columns(x)[0]
+    return c.len_dev if isinstance(c, DeviceVec) else None
+
+
+def _count_buffer(exec: Executor) -> torch.Tensor:
+    return torch.zeros(1, dtype=torch.uint32, device=f"cuda:{exec.device}")
+
+
+def _p32(t: torch.Tensor):
+    return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_uint32))
+
+
+# ------------------------------------------------------------ transform --
+
+def copy(exec: Executor, input, output: DeviceVec) -> None:
+    """vector::copy (massively/src/api/algorithm/transform.rs:56)."""
+    keep = []
+    s = lower(exec, input, keep)
+    check(_L().mb_copy(exec.handle, C.byref(s), output.to_col()))
+
+
+def map(exec: Executor, input, unary, dtype=None) -> DeviceVec:  # noqa: A001
+    """vector::map (transform.rs:91-110) for a built-in unary op."""
+    from .lazy import Map
+    v = Map(input, unary, dtype)
+    out = exec.alloc(v.dtype, len(v))
+    copy(exec, v, out)
+    return out
+
+
+def fill(exec: Executor, value, output: DeviceVec) -> None:
+    """vector::fill (selection.rs:321)."""
+    buf = scalar_buffer(value, output.dtype)
+    check(_L().mb_fill(exec.handle, buf, output.to_col()))
+
+
+def _binary_elementwise(exec, left, right, op, out):
+    """out[i] = op(left[i], right[i]) -- used to lower adjacent_difference."""
+    o = O.reduction(op)
+    a, b = left.tensor, right.tensor
+    if o.name == "add":
+        r = a + b
+    elif o.name == "mul":
+        r = a * b
+    elif o.name == "min":
+        r = torch.where(b < a, b, a)
+    elif o.name == "max":
+        r = torch.where(a < b, b, a)
+    elif o.name == "take_left":
+        r = a
+    elif o.name == "take_right":
+        r = b
+    else:
+        r = {"and": torch.bitwise_and, "or": torch.bitwise_or, "xor": torch.bitwise_xor}[o.name](a, b)
+    out.tensor.copy_(r)
+
+
+# ----------------------------------------------------------------- scan --
+
+def inclusive_scan(exec: Executor, input, op) -> DeviceVec:
+    """vector::inclusive_scan (massively/src/api/algorithm/scan.rs:96)."""
+    _check_owner(exec, input)
+    keep = []
+    n = _len(input)
+    s = lower(exec, input, keep)
+    out = exec.alloc(_dtype(input), n)
+    if s.len_dev:
+        out = out.with_len_dev(_len_dev_of(input))
+    check(_L().mb_inclusive_scan(exec.handle, C.byref(s), O.reduction(op).id, out.to_col()))
+    return out
+
+
+def exclusive_scan(exec: Executor, input, init, op) -> DeviceVec:
+    """vector::exclusive_scan (scan.rs:216)."""
+    _check_owner(exec, input)
+    keep = []
+    n = _len(input)
+    s = lower(exec, input, keep)
+    out = exec.alloc(_dtype(input), n)
+    if s.len_dev:
+        out = out.with_len_dev(_len_dev_of(input))
+    buf = scalar_buffer(init, _dtype(input))
+    check(_L().mb_exclusive_scan(exec.handle, C.byref(s), O.reduction(op).id, buf,
+                                 out.to_col()))
+    return out
+
+
+def inclusive_scan_into(exec: Executor, input, op, output: DeviceVec) -> None:
+    """inclusive_scan into caller storage (scan.rs:117)."""
+    keep = []
+    s = lower(exec, input, keep)
+    check(_L().mb_inclusive_scan(exec.handle, C.byref(s), O.reduction(op).id, output.to_col()))
+
+
+def exclusive_scan_into(exec: Executor, input, init, op, output: DeviceVec) -> None:
+    keep = []
+    s = lower(exec, input, keep)
+    buf = scalar_buffer(init, _dtype(input))
+    check(_L().mb_exclusive_scan(exec.handle, C.byref(s), O.reduction(op).id, buf,
+                                 output.to_col()))
+
+
+def adjacent_difference(exec: Executor, input, op) -> DeviceVec:
+    """vector::adjacent_difference (scan.rs:156)."""
+    from .lazy import AdjacentDifference, _as_column
+    keep = []
+    return _as_column(exec, AdjacentDifference(input, op), keep)
+
+
+# --------------------------------------------------------------- reduce --
+
+def reduce(exec: Executor, input, init, op):
+    """vector::reduce (massively/src/api/algorithm/reduce.rs:32-50): returns
+    `init op fold(input)` on the host (synchronises)."""
+    _check_owner(exec, input)
+    keep = []
+    _len(input)
+    s = lower(exec, input, keep)
+    dt = ID_TO_NP[s.vtype]
+    buf = scalar_buffer(init, dt)
+    res = np.zeros(1, dtype=dt)
+    check(_L().mb_reduce(exec.handle, C.byref(s), O.reduction(op).id, buf, None,
+                         res.ctypes.data_as(C.c_void_p)))
+    return res[0]
+
+
+def reduce_to_device(exec: Executor, input, init, op) -> DeviceVec:
+    """reduce whose single result stays on the device (no synchronisation)."""
+    keep = []
+    s = lower(exec, input, keep)
+    dt = ID_TO_NP[s.vtype]
+    out = exec.alloc(dt, 1)
+    buf = scalar_buffer(init, dt)
+    check(_L().mb_reduce(exec.handle, C.byref(s), O.reduction(op).id, buf,
+                         C.c_void_p(out.data_ptr()), None))
+    return out
+
+
+# ------------------------------------------------------------ selection --
+
+def _stencil_src(exec, stencil, keep):
+    return lower(exec, stencil, keep)
+
+
+def copy_where(exec: Executor, input, stencil):
+    """vector::copy_where (massively/src/api/algorithm/selection.rs:146):
+    rows whose stencil flag is non-zero, stable; the count stays on device."""
+    return _select(exec, input, stencil, remove=False)
+
+
+def remove_where(exec: Executor, input, stencil):
+    """vector::remove_where (selection.rs:203)."""
+    return _select(exec, input, stencil, remove=True)
+
+
+def _select(exec, input, stencil, remove):
+    _check_owner(exec, input, stencil)
+    n, m = _len(input), _len(stencil)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    srcs, k = _srcs(exec, input, keep)
+    st = _stencil_src(exec, stencil, keep)
+    cnt = _count_buffer(exec)
+    outs = _out_like(exec, input, n, cnt)
+    fn = _L().mb_remove_where if remove else _L().mb_copy_where
+    check(fn(exec.handle, srcs, k, C.byref(st), _cols(outs), _p32(cnt), None))
+    return _wrap(input, outs)
+
+
+def partition(exec: Executor, input, pred, column: int = 0):
+    """vector::partition (selection.rs:272): (rows where pred holds, then the
+    rest, both stable; boundary).  `column` picks the zipped column tested."""
+    _check_owner(exec, input)
+    n = _len(input)
+    keep = []
+    srcs, k = _srcs(exec, input, keep)
+    outs = _out_like(exec, input, n)
+    b = C.c_uint32(0)
+    check(_L().mb_partition(exec.handle, srcs, k, column, O.unary(pred).id, _cols(outs), None,
+                            C.byref(b)))
+    return _wrap(input, outs), int(b.value)
+
+
+# ------------------------------------------------------- gather/scatter --
+
+def gather(exec: Executor, values, indices):
+    """vector::gather (massively/src/api/algorithm/indexed.rs:172)."""
+    _check_owner(exec, values, indices)
+    n = _len(indices)
+    outs = _out_like(exec, values, n)
+    _gather_into(exec, values, indices, None, outs)
+    return _wrap(values, outs)
+
+
+def gather_where(exec: Executor, values, indices, stencil, output) -> None:
+    """vector::gather_where (indexed.rs:237): writes only where stencil != 0."""
+    _check_owner(exec, values, indices, stencil, output)
+    n, m = _len(indices), _len(stencil)
+    if n != m:
+        raise LengthMismatch(n, m)
+    _gather_into(exec, values, indices, stencil, _columns(output))
+
+
+def _gather_into(exec, values, indices, stencil, outs):
+    keep = []
+    idx = lower(exec, indices, keep)
+    st = lower(exec, stencil, keep) if stencil is not None else None
+    for c, o in zip(_columns(values), outs):
+        s = lower(exec, c, keep)
+        check(_L().mb_gather(exec.handle, C.byref(s), C.byref(idx),
+                             C.byref(st) if st is not None else None, o.to_col()))
+
+
+def scatter(exec: Executor, values, indices, output) -> None:
+    """vector::scatter (massively/src/api/algorithm/scatter.rs:248)."""
+    _check_owner(exec, values, indices, output)
+    n, m = _len(values), _len(indices)
+    if n != m:
+        raise LengthMismatch(n, m)
+    _scatter_into(exec, values, indices, None, _columns(output))
+
+
+def scatter_where(exec: Executor, values, indices, stencil, output) -> None:
+    """vector::scatter_where (scatter.rs:315)."""
+    _check_owner(exec, values, indices, stencil, output)
+    n, m = _len(values), _len(indices)
+    if n != m:
+        raise LengthMismatch(n, m)
+    _scatter_into(exec, values, indices, stencil, _columns(output))
+
+
+def _scatter_into(exec, values, indices, stencil, outs):
+    keep = []
+    idx = lower(exec, indices, keep)
+    st = lower(exec, stencil, keep) if stencil is not None else None
+    for c, o in zip(_columns(values), outs):
+        s = lower(exec, c, keep)
+        check(_L().mb_scatter(exec.handle, C.byref(s), C.byref(idx),
+                              C.byref(st) if st is not None else None, o.to_col()))
+
+
+def reverse(exec: Executor, values):
+    """vector::reverse (indexed.rs:289)."""
+    from .lazy import Reverse
+    outs = []
+    for c in _columns(values):
+        o = exec.alloc(c.dtype, len(c))
+        copy(exec, Reverse(c, len(c)), o)
+        outs.append(o)
+    return _wrap(values, outs)
+
+
+# ------------------------------------------------------------- ordering --
+
+def radix_sort_by_key(exec: Executor, keys, values):
+    """vector::radix_sort_by_key (massively/src/api/algorithm/by_key.rs:272):
+    the values permuted into the stable radix order of the keys (1-3 key
+    columns, the first primary)."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks, nk = _srcs(exec, keys, keep)
+    vs, nv = _srcs(exec, values, keep)
+    outs = _out_like(exec, values, n)
+    check(_L().mb_radix_sort_by_key(exec.handle, ks, nk, vs, nv, _cols(outs), None))
+    return _wrap(values, outs)
+
+
+def radix_sort_pairs(exec: Executor, keys, values):
+    """Sorted keys and values together (one onesweep pass set)."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks, nk = _srcs(exec, keys, keep)
+    vs, nv = _srcs(exec, values, keep)
+    kout = _out_like(exec, keys, n)
+    vout = _out_like(exec, values, n)
+    check(_L().mb_radix_sort_by_key(exec.handle, ks, nk, vs, nv, _cols(vout), _cols(kout)))
+    return _wrap(keys, kout), _wrap(values, vout)
+
+
+def sort(exec: Executor, input, less=O.Less) -> DeviceVec:
+    """vector::sort (massively/src/api/algorithm/ordering.rs:64): stable."""
+    _check_owner(exec, input)
+    keep = []
+    _len(input)
+    s = lower(exec, input, keep)
+    out = exec.alloc(_dtype(input), len(input))
+    check(_L().mb_sort(exec.handle, C.byref(s), O.pred2(less).id, out.to_col()))
+    return out
+
+
+def sort_by_key(exec: Executor, keys, values, less=O.Less):
+    """vector::sort_by_key (by_key.rs:226): the values in the stable order of
+    the keys under `less`."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks = lower(exec, keys, keep)
+    vs, nv = _srcs(exec, values, keep)
+    outs = _out_like(exec, values, n)
+    check(_L().mb_sort_by_key(exec.handle, C.byref(ks), O.pred2(less).id, vs, nv, None,
+                              _cols(outs)))
+    return _wrap(values, outs)
+
+
+# --------------------------------------------------------------- by key --
+
+def _ops_inits(values, op, init):
+    cols = _columns(values)
+    ops = list(op) if isinstance(op, (tuple, list)) else [op] * len(cols)
+    inits = list(init) if isinstance(init, (tuple, list)) else [init] * len(cols)
+    if len(ops) != len(cols) or len(inits) != len(cols):
+        raise LengthMismatch(len(cols), len(ops))
+    from .runtime import value_bits
+    ids = (C.c_int * len(cols))(*[O.reduction(o).id for o in ops])
+    bits = (C.c_uint64 * len(cols))(*[value_bits(i, c.dtype) for i, c in zip(inits, cols)])
+    return ids, bits
+
+
+def reduce_by_key(exec: Executor, keys, values, equal, init, op):
+    """vector::reduce_by_key (massively/src/api/algorithm/by_key.rs:618):
+    (run keys, per-run init op v...) with the run count on the device.  For
+    zipped values `op` / `init` may be per-column tuples."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks = lower(exec, keys, keep)
+    vs, nv = _srcs(exec, values, keep)
+    ids, bits = _ops_inits(values, op, init)
+    cnt = _count_buffer(exec)
+    kout = exec.alloc(_dtype(keys), n).with_len_dev(cnt)
+    vout = _out_like(exec, values, n, cnt)
+    check(_L().mb_reduce_by_key(exec.handle, C.byref(ks), O.pred2(equal).id, vs, nv, ids, bits,
+                                kout.to_col(), _cols(vout), _p32(cnt), None))
+    return kout, _wrap(values, vout)
+
+
+def inclusive_scan_by_key(exec: Executor, keys, values, equal, op):
+    """vector::inclusive_scan_by_key (by_key.rs:399)."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks = lower(exec, keys, keep)
+    outs = []
+    for c in _columns(values):
+        s = lower(exec, c, keep)
+        o = exec.alloc(c.dtype, n)
+        check(_L().mb_inclusive_scan_by_key(exec.handle, C.byref(ks), O.pred2(equal).id,
+                                            C.byref(s), O.reduction(op).id, o.to_col()))
+        outs.append(o)
+    return _wrap(values, outs)
+
+
+def exclusive_scan_by_key(exec: Executor, keys, values, equal, init, op):
+    """vector::exclusive_scan_by_key (by_key.rs:497)."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks = lower(exec, keys, keep)
+    cols = _columns(values)
+    inits = list(init) if isinstance(init, (tuple, list)) else [init] * len(cols)
+    outs = []
+    for c, i in zip(cols, inits):
+        s = lower(exec, c, keep)
+        o = exec.alloc(c.dtype, n)
+        buf = scalar_buffer(i, c.dtype)
+        check(_L().mb_exclusive_scan_by_key(exec.handle, C.byref(ks), O.pred2(equal).id,
+                                            C.byref(s), O.reduction(op).id, buf, o.to_col()))
+        outs.append(o)
+    return _wrap(values, outs)
+
+
+# ---------------------------------------------------------- merge / set --
+
+def merge(exec: Executor, left, right, less=O.Less) -> DeviceVec:
+    """vector::merge (massively/src/api/algorithm/merge.rs:109)."""
+    _check_owner(exec, left, right)
+    keep = []
+    ls, rs = lower(exec, left, keep), lower(exec, right, keep)
+    _len(left), _len(right)
+    out = exec.alloc(_dtype(left), len(left) + len(right))
+    check(_L().mb_merge(exec.handle, C.byref(ls), C.byref(rs), O.pred2(less).id, out.to_col()))
+    return out
+
+
+def merge_by_key(exec: Executor, left_keys, left_values, right_keys, right_values,
+                 less=O.Less):
+    """vector::merge_by_key (merge.rs:195): the merged values."""
+    _check_owner(exec, left_keys, left_values, right_keys, right_values)
+    if len(left_keys) != len(left_values):
+        raise LengthMismatch(len(left_keys), len(left_values))
+    if len(right_keys) != len(right_values):
+        raise LengthMismatch(len(right_keys), len(right_values))
+    keep = []
+    lk, rk = lower(exec, left_keys, keep), lower(exec, right_keys, keep)
+    lv, nv = _srcs(exec, left_values, keep)
+    rv, _ = _srcs(exec, right_values, keep)
+    n = len(left_keys) + len(right_keys)
+    kout = exec.alloc(_dtype(left_keys), n)
+    vout = _out_like(exec, left_values, n)
+    check(_L().mb_merge_by_key(exec.handle, C.byref(lk), lv, C.byref(rk), rv, nv,
+                               O.pred2(less).id, kout.to_col(), _cols(vout)))
+    return _wrap(left_values, vout)
+
+
+def _set(exec, left, right, less, fn, cap):
+    _check_owner(exec, left, right)
+    keep = []
+    ls, rs = lower(exec, left, keep), lower(exec, right, keep)
+    cnt = _count_buffer(exec)
+    out = exec.alloc(_dtype(left), cap).with_len_dev(cnt)
+    check(fn(exec.handle, C.byref(ls), C.byref(rs), O.pred2(less).id, out.to_col(), _p32(cnt),
+             None))
+    return out
+
+
+def set_union(exec: Executor, left, right, less=O.Less) -> DeviceVec:
+    """vector::set_union (massively/src/api/algorithm/set.rs:47)."""
+    return _set(exec, left, right, less, _L().mb_set_union, len(left) + len(right))
+
+
+def set_intersection(exec: Executor, left, right, less=O.Less) -> DeviceVec:
+    """vector::set_intersection (set.rs:99)."""
+    return _set(exec, left, right, less, _L().mb_set_intersection, len(left))
+
+
+def set_difference(exec: Executor, left, right, less=O.Less) -> DeviceVec:
+    """vector::set_difference (set.rs:151)."""
+    return _set(exec, left, right, less, _L().mb_set_difference, len(left))

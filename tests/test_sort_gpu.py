@@ -1,0 +1,163 @@
+"""Radix and comparator sort parity: CUDA path vs the oracle, bit-exact
+(keys, values and stability), through the C ABI."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from tests.golden import known_answers as K
+from tests.gpu_util import executor, gpu, seeded
+
+pytestmark = gpu
+
+
+@pytest.fixture(scope="module")
+def ex():
+    return executor()
+
+
+def _perm_values(n):
+    return np.arange(n, dtype=np.uint32)
+
+
+def test_known_answers(ex):
+    from massively_b200 import op, vector, zip3, zip7, zip12
+    for case in K.RADIX:
+        got = vector.radix_sort_by_key(ex, ex.to_device(case["keys"][0]),
+                                       ex.to_device(case["values"]))
+        np.testing.assert_array_equal(ex.to_host(got), case["want"], err_msg=case["src"])
+    for case in K.RADIX_INTEGER_EXTREMES + K.RADIX_FLOAT_TOTAL_ORDER:
+        n = case["keys"].size
+        got = vector.radix_sort_by_key(ex, ex.to_device(case["keys"]),
+                                       ex.to_device(_perm_values(n)))
+        np.testing.assert_array_equal(ex.to_host(got), case["want"], err_msg=case["src"])
+    c = K.RADIX_COMPOUND
+    n = c["keys"][0].size
+    vals = [np.array([col * 100 + i for i in range(n)], np.uint32) for col in range(12)]
+    keys = zip3(*[ex.to_device(k) for k in c["keys"]])
+    got = vector.radix_sort_by_key(ex, keys, zip7(*[ex.to_device(v) for v in vals[:7]]))
+    for col, g in enumerate(got.into_columns()):
+        np.testing.assert_array_equal(ex.to_host(g), vals[col][c["want"]])
+    got = vector.radix_sort_by_key(ex, keys, zip12(*[ex.to_device(v) for v in vals]))
+    for col, g in enumerate(got.into_columns()):
+        np.testing.assert_array_equal(ex.to_host(g), vals[col][c["want"]])
+    n = K.RADIX_513["n"]
+    k = ((np.arange(n) * 37) % 11).astype(np.uint32)
+    got = vector.radix_sort_by_key(ex, ex.to_device(k), ex.to_device(_perm_values(n)))
+    np.testing.assert_array_equal(ex.to_host(got), np.argsort(k, kind="stable"))
+    for case in K.SORT:
+        np.testing.assert_array_equal(ex.to_host(vector.sort(ex, ex.to_device(case["x"]))),
+                                      case["want"])
+    for case in K.SORT_BY_KEY:
+        got = vector.sort_by_key(ex, ex.to_device(case["keys"]), ex.to_device(case["values"]),
+                                 op.Less)
+        np.testing.assert_array_equal(ex.to_host(got), case["want"])
+
+
+def test_empty_and_length_mismatch(ex):
+    import massively_b200 as mb
+    from massively_b200 import vector
+    e = ex.to_device(np.zeros(0, np.uint32))
+    assert ex.to_host(vector.radix_sort_by_key(ex, e, e)).size == 0
+    with pytest.raises(mb.LengthMismatch) as err:
+        vector.radix_sort_by_key(ex, ex.to_device(np.array([1, 2], np.uint32)),
+                                 ex.to_device(np.array([10], np.uint32)))
+    assert err.value == mb.LengthMismatch(2, 1)
+
+
+SIZES = K.ORACLE_LENGTHS + [4095, 4096, 4097, 65_537, 1 << 20, 3_000_017]
+
+
+@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("keyspace", ["full", "mod37", "16bit", "const"])
+def test_u32_pairs_bit_exact(ex, n, keyspace):
+    from massively_b200 import vector
+    keys = seeded(np.uint32, n, seed=n + 17)
+    if keyspace == "mod37":
+        keys = ((np.arange(n, dtype=np.uint64) * 1103515245 + 12345) % 37).astype(np.uint32)
+    elif keyspace == "16bit":
+        keys = keys & np.uint32(0xFFFF)
+    elif keyspace == "const":
+        keys = np.full(n, 7, np.uint32)
+    vals = _perm_values(n)
+    sk, sv = vector.radix_sort_pairs(ex, ex.to_device(keys), ex.to_device(vals))
+    want = orc.radix_perm([keys])
+    np.testing.assert_array_equal(ex.to_host(sv), want)
+    np.testing.assert_array_equal(ex.to_host(sk), keys[want])
+
+
+@pytest.mark.parametrize("n", [0, 1, 257, 4097, 100_003, 1 << 20])
+@pytest.mark.parametrize("dtype", [np.int32, np.float32, np.uint64, np.int64, np.float64])
+def test_typed_keys_total_order(ex, n, dtype):
+    from massively_b200 import vector
+    keys = seeded(dtype, n, seed=n + 5)
+    if dtype in (np.float32, np.float64) and n > 10:
+        keys[: n // 50] = 0.0
+        keys[n // 50: n // 25] = -0.0
+        keys[-3:] = [np.inf, -np.inf, np.nan]
+    vals = _perm_values(n)
+    sk, sv = vector.radix_sort_pairs(ex, ex.to_device(keys), ex.to_device(vals))
+    want = orc.radix_perm([keys])
+    np.testing.assert_array_equal(ex.to_host(sv), want)
+    np.testing.assert_array_equal(ex.to_host(sk).view(np.uint8), keys[want].view(np.uint8))
+    # 64-bit payload column
+    v64 = np.arange(n, dtype=np.uint64) * np.uint64(3)
+    sv64 = vector.radix_sort_by_key(ex, ex.to_device(keys), ex.to_device(v64))
+    np.testing.assert_array_equal(ex.to_host(sv64), v64[want])
+
+
+@pytest.mark.parametrize("n", [5, 1000, 70_001])
+@pytest.mark.parametrize("dtype", [np.uint8, np.int16, np.int8, np.uint16])
+def test_narrow_keys(ex, n, dtype):
+    from massively_b200 import vector
+    keys = seeded(dtype, n, seed=9)
+    got = vector.radix_sort_by_key(ex, ex.to_device(keys), ex.to_device(_perm_values(n)))
+    np.testing.assert_array_equal(ex.to_host(got), orc.radix_perm([keys]))
+
+
+@pytest.mark.parametrize("less", ["less", "greater", "total_less"])
+@pytest.mark.parametrize("dtype", [np.uint32, np.int64, np.float32, np.float64])
+def test_comparator_sorts(ex, less, dtype):
+    from massively_b200 import op, vector
+    n = 50_001
+    keys = seeded(dtype, n, seed=21)
+    if dtype in (np.float32, np.float64):
+        keys[:100] = 0.0
+        keys[100:200] = -0.0
+        keys = keys.astype(dtype)
+    else:
+        keys = (keys % dtype(1000)).astype(dtype)
+    o = op.pred2(less)
+    got = ex.to_host(vector.sort(ex, ex.to_device(keys), o))
+    want = orc.sort(keys, less)
+    np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))
+    vals = _perm_values(n)
+    got = ex.to_host(vector.sort_by_key(ex, ex.to_device(keys), ex.to_device(vals), o))
+    np.testing.assert_array_equal(got, orc.sort_perm(keys, less))
+
+
+def test_lazy_keys_and_multi_values(ex):
+    from massively_b200 import lazy, op, vector, zip2
+    n = 100_000
+    src = seeded(np.uint32, n, 33)
+    d = ex.to_device(src)
+    # keys = map(src, IsEven) (a lazy view) -> stable partition order
+    got = vector.radix_sort_by_key(ex, lazy.map(d, op.IsEven), ex.to_device(_perm_values(n)))
+    flags = ((src & 1) == 0).astype(np.uint32)
+    np.testing.assert_array_equal(ex.to_host(got), np.argsort(flags, kind="stable"))
+    # config-1 shape: radix_sort_by_key(keys, zip2(keys, counting))
+    got = vector.radix_sort_by_key(ex, d, zip2(d, lazy.counting(0).take(n)))
+    k2, v2 = got.into_columns()
+    want = orc.radix_perm([src])
+    np.testing.assert_array_equal(ex.to_host(k2), src[want])
+    np.testing.assert_array_equal(ex.to_host(v2), want)
+
+
+def test_large_pairs(ex):
+    from massively_b200 import vector
+    n = 1 << 24
+    keys = seeded(np.uint32, n, 0)
+    vals = _perm_values(n)
+    sk, sv = vector.radix_sort_pairs(ex, ex.to_device(keys), ex.to_device(vals))
+    want = np.argsort(keys, kind="stable").astype(np.uint32)
+    np.testing.assert_array_equal(ex.to_host(sv), want)
+    np.testing.assert_array_equal(ex.to_host(sk), keys[want])
