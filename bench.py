@@ -307,13 +307,21 @@ class SortU64(Workload):
         return self.n * n_gpus / (ms * 1e-3) / 1e9
 
 
+def _n(default_log2: int) -> int:
+    """Items of a workload: its configured size, or 2^MB_BENCH_LOG2N for
+    small profiling captures of the same kernels."""
+    v = os.environ.get("MB_BENCH_LOG2N")
+    return 1 << (int(v) if v else default_log2)
+
+
 WORKLOADS = {
-    "sort_pairs_u32": lambda: SortPairsU32(),
-    "sort_pairs_u32_16bit": lambda: SortPairsU32(key_hi=65535, seed=1, tag="_keys2^16"),
-    "scan_u32": lambda: ScanU32(),
-    "scan_f32": lambda: ScanF32(),
-    "copy_where_u32": lambda: CopyWhereU32(),
-    "sort_u64": lambda: SortU64(),
+    "sort_pairs_u32": lambda: SortPairsU32(n=_n(28)),
+    "sort_pairs_u32_16bit": lambda: SortPairsU32(n=_n(28), key_hi=65535, seed=1,
+                                                 tag="_keys2^16"),
+    "scan_u32": lambda: ScanU32(n=_n(30)),
+    "scan_f32": lambda: ScanF32(n=_n(28)),
+    "copy_where_u32": lambda: CopyWhereU32(n=_n(28)),
+    "sort_u64": lambda: SortU64(n=_n(27)),
 }
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64"]
 

@@ -315,14 +315,28 @@ __device__ __forceinline__ void raise_device_error(uint32_t* status, uint32_t co
   if (status) atomicCAS(status, 0u, code);
 }
 
+// Where a kernel reports a failure: the executor's status word (read by
+// mb_sync) and a per-launch abort word (zeroed with the launch's scratch) that
+// tells the other waiting blocks of the same launch to stop waiting.
+struct DevErr {
+  uint32_t* status;
+  uint32_t* abort;
+};
+
+__device__ __forceinline__ void raise_device_error(DevErr e, uint32_t code) {
+  if (e.status) atomicCAS(e.status, 0u, code);
+  if (e.abort) atomicExch(e.abort, 1u);
+}
+
 // Bounded-wait bookkeeping for one spinning thread.  `expired()` is true
-// once the wait passed kSpinLimitNs or another block already failed.
+// once the wait passed kSpinLimitNs or another block of the same launch
+// already gave up.
 struct SpinGuard {
   uint64_t start;
   uint32_t iter;
   const uint32_t* status;
-  __device__ __forceinline__ explicit SpinGuard(const uint32_t* st)
-      : start(0), iter(0), status(st) {}
+  __device__ __forceinline__ explicit SpinGuard(const uint32_t* abort_word)
+      : start(0), iter(0), status(abort_word) {}
   __device__ __forceinline__ bool expired() {
     ++iter;
     if ((iter & 63u) != 0) return false;

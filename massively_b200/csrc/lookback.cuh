@@ -1,16 +1,17 @@
 // lookback.cuh -- tile status words and the warp-wide decoupled look-back
-// used by every single-pass kernel (scan, compaction, segmented scan,
-// reduce_by_key).
+// used by every single-pass kernel (scan, compaction, segmented scan and
+// reduce, by-key algorithms).
 //
 // A tile publishes its aggregate (flag 1) as soon as it has reduced its own
 // items, then its inclusive prefix (flag 2) once it knows its exclusive
 // prefix.  Its successors look back over a window of 32 predecessors.
 //
 // Two publication layouts:
-//  * packed: 32-bit values, flag and value in one 64-bit word written with a
+//  * packed: 4-byte values, flag and value in one 64-bit word written with a
 //    single relaxed store (one load per predecessor on the read side);
 //  * split: flag word (release / acquire) + separate aggregate and inclusive
-//    arrays, for 64-bit values.
+//    arrays, for wider values (8 and 16 bytes: 64-bit values, and the
+//    (head count, value) pairs of the segmented kernels).
 //
 // Deterministic mode (floating point): the exclusive prefix of tile t is the
 // left fold P(j) op A(j+1) op ... op A(t-1) starting from the nearest
@@ -21,7 +22,8 @@
 // window with a warp tree instead.
 //
 // Every wait is bounded (SpinGuard): on expiry the tile records
-// MB_DEV_ERR_LOOKBACK and continues with a zero prefix so the launch ends.
+// MB_DEV_ERR_LOOKBACK and continues with a fallback prefix so the launch
+// ends; the host reports MB_ERR_LAUNCH at the next synchronisation.
 #pragma once
 
 #include "common.cuh"
@@ -33,6 +35,7 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 
 template <class T>
 __device__ __forceinline__ uint64_t to_bits64(T v) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte value");
   if constexpr (sizeof(T) == 4) {
     uint32_t b;
     memcpy(&b, &v, 4);
@@ -55,29 +58,66 @@ __device__ __forceinline__ T from_bits64(uint64_t b) {
   return v;
 }
 
+// Word-wise warp shuffles of any trivially copyable T (size multiple of 4).
 template <class T>
 __device__ __forceinline__ T shfl_idx(T v, int src) {
-  if constexpr (sizeof(T) == 4) {
-    return from_bits64<T>((uint32_t)__shfl_sync(kFull, (uint32_t)to_bits64(v), src));
-  } else {
-    return from_bits64<T>((uint64_t)__shfl_sync(kFull, (unsigned long long)to_bits64(v), src));
-  }
+  static_assert(sizeof(T) % 4 == 0, "size must be a multiple of 4");
+  uint32_t w[sizeof(T) / 4];
+  memcpy(w, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 4); ++i) w[i] = __shfl_sync(kFull, w[i], src);
+  memcpy(&v, w, sizeof(T));
+  return v;
 }
 template <class T>
 __device__ __forceinline__ T shfl_up(T v, int d) {
-  if constexpr (sizeof(T) == 4) {
-    return from_bits64<T>((uint32_t)__shfl_up_sync(kFull, (uint32_t)to_bits64(v), d));
-  } else {
-    return from_bits64<T>((uint64_t)__shfl_up_sync(kFull, (unsigned long long)to_bits64(v), d));
-  }
+  uint32_t w[sizeof(T) / 4];
+  memcpy(w, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 4); ++i) w[i] = __shfl_up_sync(kFull, w[i], d);
+  memcpy(&v, w, sizeof(T));
+  return v;
 }
 template <class T>
 __device__ __forceinline__ T shfl_down(T v, int d) {
-  if constexpr (sizeof(T) == 4) {
-    return from_bits64<T>((uint32_t)__shfl_down_sync(kFull, (uint32_t)to_bits64(v), d));
+  uint32_t w[sizeof(T) / 4];
+  memcpy(w, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 4); ++i) w[i] = __shfl_down_sync(kFull, w[i], d);
+  memcpy(&v, w, sizeof(T));
+  return v;
+}
+
+// Relaxed word-wise copies to / from global memory.
+template <class T>
+__device__ __forceinline__ void st_relaxed_any(T* dst, const T& v) {
+  if constexpr (sizeof(T) % 8 == 0) {
+    uint64_t w[sizeof(T) / 8];
+    memcpy(w, &v, sizeof(T));
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 8); ++i) st_relaxed_u64((uint64_t*)dst + i, w[i]);
   } else {
-    return from_bits64<T>((uint64_t)__shfl_down_sync(kFull, (unsigned long long)to_bits64(v), d));
+    uint32_t w[sizeof(T) / 4];
+    memcpy(w, &v, sizeof(T));
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 4); ++i) st_relaxed_u32((uint32_t*)dst + i, w[i]);
   }
+}
+template <class T>
+__device__ __forceinline__ T ld_relaxed_any(const T* src) {
+  T v;
+  if constexpr (sizeof(T) % 8 == 0) {
+    uint64_t w[sizeof(T) / 8];
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 8); ++i) w[i] = ld_relaxed_u64((const uint64_t*)src + i);
+    memcpy(&v, w, sizeof(T));
+  } else {
+    uint32_t w[sizeof(T) / 4];
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 4); ++i) w[i] = ld_relaxed_u32((const uint32_t*)src + i);
+    memcpy(&v, w, sizeof(T));
+  }
+  return v;
 }
 
 // Status storage of one launch.  `words` (packed) or `flags`/`agg`/`incl`.
@@ -105,14 +145,10 @@ struct TileState {
   }
   __device__ __forceinline__ void publish(uint64_t t, uint32_t flag, T v) const {
     if constexpr (PACKED) {
+      static_assert(sizeof(T) == 4, "packed layout holds 4-byte values");
       st_relaxed_u64(words + t, ((uint64_t)flag << 32) | to_bits64(v));
     } else {
-      T* dst = flag == kFlagAgg ? agg : incl;
-      if constexpr (sizeof(T) == 4) {
-        st_relaxed_u32((uint32_t*)(dst + t), (uint32_t)to_bits64(v));
-      } else {
-        st_relaxed_u64((uint64_t*)(dst + t), to_bits64(v));
-      }
+      st_relaxed_any((flag == kFlagAgg ? agg : incl) + t, v);
       st_release_u32(flags + t, flag);
     }
   }
@@ -124,23 +160,8 @@ struct TileState {
       return (uint32_t)(w >> 32);
     } else {
       uint32_t f = ld_acquire_u32(flags + t);
-      if (f != kFlagNone) {
-        const T* src = f == kFlagAgg ? agg : incl;
-        if constexpr (sizeof(T) == 4) {
-          v = from_bits64<T>(ld_relaxed_u32((const uint32_t*)(src + t)));
-        } else {
-          v = from_bits64<T>(ld_relaxed_u64((const uint64_t*)(src + t)));
-        }
-      }
+      if (f != kFlagNone) v = ld_relaxed_any((f == kFlagAgg ? agg : incl) + t);
       return f;
-    }
-  }
-  // Aggregate of tile t (split layout only; valid once its flag is >= 1).
-  __device__ __forceinline__ T aggregate(uint64_t t) const {
-    if constexpr (sizeof(T) == 4) {
-      return from_bits64<T>(ld_relaxed_u32((const uint32_t*)(agg + t)));
-    } else {
-      return from_bits64<T>(ld_relaxed_u64((const uint64_t*)(agg + t)));
     }
   }
 };
@@ -163,9 +184,9 @@ __device__ __forceinline__ bool wait_window(const State& st, int64_t p, bool val
 // error and returns `fallback`.
 template <class T, class OpT, bool DET, class State>
 __device__ T lookback_exclusive(const State& st, uint64_t tile, const OpT& op,
-                                uint32_t* status_dev, T fallback) {
+                                DevErr err, T fallback) {
   const int lane = (int)lane_id();
-  SpinGuard guard(status_dev);
+  SpinGuard guard(err.abort);
   if constexpr (!DET) {
     bool have = false;
     T acc = fallback;
@@ -176,7 +197,7 @@ __device__ T lookback_exclusive(const State& st, uint64_t tile, const OpT& op,
       uint32_t f;
       T v = fallback;
       if (!wait_window<T>(st, p, valid, f, v, guard)) {
-        raise_device_error(status_dev, MB_DEV_ERR_LOOKBACK);
+        raise_device_error(err, MB_DEV_ERR_LOOKBACK);
         return fallback;
       }
       const uint32_t incl_mask = __ballot_sync(kFull, valid && f == kFlagIncl);
@@ -213,7 +234,7 @@ __device__ T lookback_exclusive(const State& st, uint64_t tile, const OpT& op,
       uint32_t f;
       T v = fallback;
       if (!wait_window<T>(st, p, valid, f, v, guard)) {
-        raise_device_error(status_dev, MB_DEV_ERR_LOOKBACK);
+        raise_device_error(err, MB_DEV_ERR_LOOKBACK);
         return fallback;
       }
       const uint32_t incl_mask = __ballot_sync(kFull, valid && f == kFlagIncl);

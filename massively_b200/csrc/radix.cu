@@ -172,7 +172,7 @@ template <class K, class V, int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS)
     radix_onesweep_kernel(const PassPlan* __restrict__ plan, int pass, uint64_t n,
                           const uint32_t* __restrict__ digit_offsets, uint32_t* __restrict__ status,
-                          uint32_t* __restrict__ counter, uint32_t* __restrict__ err) {
+                          uint32_t* __restrict__ counter, DevErr err) {
   constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
   using S = OnesweepSmem<K, V, THREADS, ITEMS>;
   constexpr int WARPS = S::WARPS;
@@ -286,19 +286,31 @@ __global__ void __launch_bounds__(THREADS)
   if (tid < kBins) {
     uint32_t excl = 0;
     if (tile > 0) {
-      SpinGuard guard(err);
-      int64_t t = (int64_t)tile - 1;
-      bool failed = false;
-      while (t >= 0) {
-        const uint32_t w = ld_relaxed_u32(status + (uint64_t)t * kBins + tid);
-        const uint32_t f = w >> 30;
-        if (f == kFlagNone) {
-          if (guard.expired()) { failed = true; break; }
-          continue;
+      // Eight predecessors per step, loaded independently, then folded in
+      // order until the first inclusive count (or an unpublished tile, which
+      // is polled again).
+      constexpr int kBatch = 8;
+      SpinGuard guard(err.abort);
+      int64_t t = (int64_t)tile - 1;  // next predecessor to account for
+      bool failed = false, done = false;
+      while (!done) {
+        uint32_t w[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j)
+          w[j] = t - j >= 0 ? ld_relaxed_u32(status + (uint64_t)(t - j) * kBins + tid)
+                            : (kFlagIncl << 30);
+        int used = 0;
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+          if (done || used < j) break;
+          const uint32_t f = w[j] >> 30;
+          if (f == kFlagNone) break;
+          excl += w[j] & kCountMask;
+          ++used;
+          if (f == kFlagIncl) done = true;
         }
-        excl += w & kCountMask;
-        if (f == kFlagIncl) break;
-        --t;
+        t -= used;
+        if (!done && used < kBatch && guard.expired()) { failed = true; break; }
       }
       if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
       st_relaxed_u32(status + tile * kBins + tid, (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
@@ -397,7 +409,8 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int p = 0; p < PASSES; ++p) {
     kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(plan, p, n, hist, status + (size_t)p * tiles * kBins,
-                                                         counters + p, ex->status_dev);
+                                                         counters + p,
+                                                         DevErr{ex->status_dev, counters + 32});
     MB_CUDA(cudaGetLastError());
   }
   return MB_OK;

@@ -44,7 +44,7 @@ struct ScanParams {
   int out_dtype;
   T init;
   uint32_t* counter;
-  uint32_t* status;
+  DevErr err;
 };
 
 template <class T>
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kThreads)
       if (lane == 0) st.publish(0, kFlagIncl, agg);
     } else {
       if (lane == 0) st.publish(tile, kFlagAgg, agg);
-      T excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.status, agg);
+      T excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.err, agg);
       if (lane == 0) {
         st.publish(tile, kFlagIncl, op(excl, agg));
         s_excl = excl;
@@ -228,7 +228,7 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
   p.init = T(0);
   if (exclusive) memcpy(&p.init, init, sizeof(T));
   p.counter = scratch.as<uint32_t>();
-  p.status = ex->status_dev;
+  p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
   auto st = TileState<T, PACKED>::make(scratch.as<char>() + 256, tiles);
   const bool plain = src_plain(in, DTypeOf<T>::value) && out.dtype == DTypeOf<T>::value &&
                      ((uintptr_t)in.data % 16 == 0) && ((uintptr_t)out.data % 16 == 0);

@@ -1,0 +1,655 @@
+// segmented.cu -- single-pass segmented scan / reduce over a Segmentation,
+// and the by-key algorithms (inclusive / exclusive scan_by_key,
+// reduce_by_key), plus Segmentation construction kernels.
+//
+// Replaces massively's head-flag pipeline (massively/src/seg/control.rs:
+// 223-285 heads fill + mark; massively/src/core/segmented_fixed.rs:22-707
+// block segmented scan, recursive segmented prefix, exclusive fix-up and the
+// per-segment tail pick; massively/src/seg/mod.rs:712-785 fill-with-init,
+// selection scan and scatter of the per-head results; massively/src/core/
+// by_key.rs:79-121 for reduce_by_key) with one kernel per call.
+//
+// Each tile marks its segment heads in a shared-memory bitmap -- from the
+// offsets (binary search for the tile's first segment, then one read per
+// segment start) or, for the by-key algorithms, from adjacent key
+// inequality -- and scans (head count, value) pairs under the segmented
+// operator  (ha, a) . (hb, b) = (ha + hb, hb ? b : a op b),  which is
+// associative, so the decoupled look-back of lookback.cuh carries segment
+// boundaries across tiles.  Reductions stage the tile's inclusive pairs in
+// shared memory and write one value per segment tail: init op inclusive
+// (massively's init op v_head ... op v_tail); empty segments get init
+// (massively/src/seg/mod.rs:728-729); run indices of reduce_by_key are the
+// inclusive head counts, and the run count stays on the device.
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "dispatch.cuh"
+#include "lookback.cuh"
+
+namespace mb {
+
+int materialize(mb_executor* ex, const mb_src& in, void* dst);
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kLoads = 4;
+
+enum SegMode : int { kScanIncl = 0, kScanExcl = 1, kReduce = 2 };
+enum HeadsSrc : int { kHeadsOffsets = 0, kHeadsKeys = 1 };
+
+template <class V>
+struct SegVal {
+  uint32_t heads;
+  V v;
+};
+
+template <class V, int OP>
+struct SegOp {
+  Op<V, OP> op;
+  __device__ __forceinline__ SegVal<V> operator()(const SegVal<V>& a, const SegVal<V>& b) const {
+    SegVal<V> r;
+    r.heads = a.heads + b.heads;
+    r.v = b.heads ? b.v : op(a.v, b.v);
+    return r;
+  }
+};
+
+template <class V>
+struct SegCfg {
+  static constexpr int VEC = 16 / sizeof(V);
+  static constexpr int ITEMS = VEC * kLoads;
+  static constexpr int WARP_ITEMS = 32 * ITEMS;
+  static constexpr int TILE = kThreads * ITEMS;
+};
+
+template <class V>
+struct SegParams {
+  int op;
+  int mode;
+  int heads_src;
+  int out_dtype;
+  V init;
+  const uint32_t* offsets;  // nseg + 1 entries
+  uint64_t nseg;
+  Src keys;
+  void* out;
+  void* out_keys;
+  int out_key_esize;
+  uint32_t* count_dev;
+  uint32_t* counter;
+  DevErr err;
+};
+
+__device__ __forceinline__ bool key_eq(int dtype, uint64_t a, uint64_t b) {
+  if (dtype == MB_F32) return __uint_as_float((uint32_t)a) == __uint_as_float((uint32_t)b);
+  if (dtype == MB_F64) return __longlong_as_double((long long)a) == __longlong_as_double((long long)b);
+  return a == b;
+}
+
+// First index in [0, count) with offsets[idx] >= x (count if none).
+__device__ __forceinline__ uint64_t lower_bound_u32(const uint32_t* a, uint64_t count, uint64_t x) {
+  uint64_t lo = 0, hi = count;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if ((uint64_t)a[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+// First index in [0, count) with offsets[idx] > x.
+__device__ __forceinline__ uint64_t upper_bound_u32(const uint32_t* a, uint64_t count, uint64_t x) {
+  uint64_t lo = 0, hi = count;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if ((uint64_t)a[mid] <= x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void st_raw_bits(void* p, uint64_t i, int esize, uint64_t bits) {
+  switch (esize) {
+    case 1: ((uint8_t*)p)[i] = (uint8_t)bits; break;
+    case 2: ((uint16_t*)p)[i] = (uint16_t)bits; break;
+    case 4: ((uint32_t*)p)[i] = (uint32_t)bits; break;
+    default: ((uint64_t*)p)[i] = bits; break;
+  }
+}
+
+template <class V, int OP, bool PLAIN>
+__global__ void __launch_bounds__(kThreads)
+    seg_kernel(Src in, uint64_t cap, SegParams<V> p, TileState<SegVal<V>, false> st) {
+  using C = SegCfg<V>;
+  using T = SegVal<V>;
+  constexpr int VEC = C::VEC;
+  constexpr bool DET = std::is_floating_point<V>::value;
+  extern __shared__ __align__(16) unsigned char seg_smem[];
+  T* stage = reinterpret_cast<T*>(seg_smem);  // kReduce only: TILE entries
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_bits[C::TILE / 32];
+  __shared__ T s_warp_total[kWarps];
+  __shared__ T s_excl;
+  __shared__ uint64_t s_seg[3];  // continuing segment, first start, end
+  __shared__ uint32_t s_head_te;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) s_tile = atomicAdd(p.counter, 1u);
+  for (int w = tid; w < C::TILE / 32; w += kThreads) s_bits[w] = 0;
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t n = in.len_dev ? min((uint64_t)*in.len_dev, cap) : cap;
+  const uint64_t tb = tile * (uint64_t)C::TILE;
+  if (tb >= n) return;
+  const uint64_t te = min(tb + (uint64_t)C::TILE, n);
+  const bool last_tile = te == n;
+
+  // ---- heads ----
+  if (p.heads_src == kHeadsOffsets) {
+    if (tid == 0) {
+      const uint64_t cnt = p.nseg + 1;
+      const uint64_t sc = upper_bound_u32(p.offsets, cnt, tb) - 1;  // segment holding tb
+      const uint64_t sa = lower_bound_u32(p.offsets, cnt, tb);      // first start >= tb
+      const uint64_t sb = last_tile ? p.nseg : min(lower_bound_u32(p.offsets, cnt, te), p.nseg);
+      s_seg[0] = (sc < p.nseg && p.offsets[sc] < tb) ? sc : ~0ull;
+      s_seg[1] = sa;
+      s_seg[2] = sb;
+    }
+    __syncthreads();
+    for (uint64_t s = s_seg[1] + tid; s < s_seg[2]; s += kThreads) {
+      const uint64_t start = p.offsets[s];
+      if (start >= tb && start < te) atomicOr(&s_bits[(start - tb) >> 5], 1u << ((start - tb) & 31));
+    }
+  } else {
+    for (uint64_t i = tb + tid; i < te; i += kThreads) {
+      bool h = i == 0;
+      if (!h) h = !key_eq(p.keys.vtype, src_load_bits(p.keys, i - 1), src_load_bits(p.keys, i));
+      if (h) atomicOr(&s_bits[(i - tb) >> 5], 1u << ((i - tb) & 31));
+    }
+    if (tid == 0)
+      s_head_te = te < n ? !key_eq(p.keys.vtype, src_load_bits(p.keys, te - 1),
+                                   src_load_bits(p.keys, te))
+                         : 1u;
+  }
+  __syncthreads();
+
+  // ---- load (value, head) pairs ----
+  const SegOp<V, OP> op{Op<V, OP>{p.op}};
+  const int warp = tid >> 5, lane = tid & 31;
+  const uint64_t warp_base = tb + (uint64_t)warp * C::WARP_ITEMS;
+  const bool full = tb + C::TILE <= n;
+  T x[kLoads][VEC];
+  {
+    V raw[kLoads][VEC];
+    if (PLAIN && full) {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j) {
+        uint4 u = __ldcs(reinterpret_cast<const uint4*>((const V*)in.data +
+                                                        warp_base + (uint64_t)(j * 32 + lane) * VEC));
+        memcpy(raw[j], &u, 16);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
+          if (i < n) {
+            if constexpr (PLAIN) raw[j][k] = ((const V*)in.data)[i];
+            else raw[j][k] = src_load<V>(in, i);
+          } else {
+            raw[j][k] = V(0);
+          }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) {
+        const uint32_t pos = (uint32_t)(warp_base - tb) + (j * 32 + lane) * VEC + k;
+        x[j][k].v = raw[j][k];
+        x[j][k].heads = (s_bits[pos >> 5] >> (pos & 31)) & 1u;
+      }
+  }
+
+  // ---- tile scan (same structure as the plain scan kernel) ----
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+    for (int k = 1; k < VEC; ++k) x[j][k] = op(x[j][k - 1], x[j][k]);
+  T ge[kLoads], rowtot[kLoads];
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j) {
+    T g = x[j][VEC - 1];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      T o = shfl_up(g, d);
+      if (lane >= d) g = op(o, g);
+    }
+    rowtot[j] = shfl_idx(g, 31);
+    ge[j] = shfl_up(g, 1);
+  }
+  T rp[kLoads];
+  rp[0] = rowtot[0];
+#pragma unroll
+  for (int j = 1; j < kLoads; ++j) rp[j] = op(rp[j - 1], rowtot[j]);
+  if (lane == 0) s_warp_total[warp] = rp[kLoads - 1];
+  __syncthreads();
+  if (warp == 0) {
+    T agg = s_warp_total[0];
+#pragma unroll
+    for (int w = 1; w < kWarps; ++w) agg = op(agg, s_warp_total[w]);
+    if (tile == 0) {
+      if (lane == 0) st.publish(0, kFlagIncl, agg);
+    } else {
+      if (lane == 0) st.publish(tile, kFlagAgg, agg);
+      T excl = lookback_exclusive<T, SegOp<V, OP>, DET>(st, tile, op, p.err, agg);
+      if (lane == 0) {
+        st.publish(tile, kFlagIncl, op(excl, agg));
+        s_excl = excl;
+      }
+    }
+  }
+  __syncthreads();
+  bool has_pre = tile > 0;
+  T pre = has_pre ? s_excl : T{0, V(0)};
+  for (int w = 0; w < warp; ++w) {
+    T t = s_warp_total[w];
+    pre = has_pre ? op(pre, t) : t;
+    has_pre = true;
+  }
+  T y[kLoads][VEC];
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j) {
+    bool h = has_pre;
+    T pj = pre;
+    if (j > 0) { pj = h ? op(pj, rp[j - 1]) : rp[j - 1]; h = true; }
+    if (lane > 0) { pj = h ? op(pj, ge[j]) : ge[j]; h = true; }
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) y[j][k] = h ? op(pj, x[j][k]) : x[j][k];
+  }
+
+  const Op<V, OP> vop{p.op};
+  if (p.mode == kScanIncl || p.mode == kScanExcl) {
+    V o[kLoads][VEC];
+    if (p.mode == kScanIncl) {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) o[j][k] = y[j][k].v;
+    } else {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j) {
+        V up = shfl_up(y[j][VEC - 1].v, 1);
+        V wrap = shfl_idx(j > 0 ? y[j - 1][VEC - 1].v : y[0][VEC - 1].v, 31);
+        const V prev0 = lane > 0 ? up : (j > 0 ? wrap : pre.v);
+        // A head restarts at init; any other item is init op inclusive of
+        // the item before it (which lies in the same segment).
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          const uint32_t pos = (uint32_t)(warp_base - tb) + (j * 32 + lane) * VEC + k;
+          const bool hd = ((s_bits[pos >> 5] >> (pos & 31)) & 1u) || tb + pos == 0;
+          const V prev = k == 0 ? prev0 : y[j][k - 1].v;
+          o[j][k] = hd ? p.init : vop(p.init, prev);
+        }
+      }
+    }
+    if (PLAIN && full && p.out_dtype == DTypeOf<V>::value) {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j) {
+        uint4 u;
+        memcpy(&u, o[j], 16);
+        __stcs(reinterpret_cast<uint4*>((V*)p.out + warp_base + (uint64_t)(j * 32 + lane) * VEC), u);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
+          if (i < n) st_cast<V>(p.out_dtype, p.out, i, o[j][k]);
+        }
+    }
+    return;
+  }
+
+  // ---- reductions: stage inclusive pairs, write one value per tail ----
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) {
+      const uint32_t pos = (uint32_t)(warp_base - tb) + (j * 32 + lane) * VEC + k;
+      stage[pos] = y[j][k];
+    }
+  __syncthreads();
+  if (p.heads_src == kHeadsOffsets) {
+    // Segment s is written by the tile holding its tail (non-empty) or its
+    // start (empty; the last tile takes starts at n).
+    auto write_seg = [&](uint64_t s) {
+      const uint64_t start = p.offsets[s], end = p.offsets[s + 1];
+      if (start == end) {
+        if ((start >= tb && start < te) || (last_tile && start >= te))
+          st_cast<V>(p.out_dtype, p.out, s, p.init);
+      } else if (end - 1 >= tb && end - 1 < te) {
+        st_cast<V>(p.out_dtype, p.out, s, vop(p.init, stage[end - 1 - tb].v));
+      }
+    };
+    if (tid == 0 && s_seg[0] != ~0ull) write_seg(s_seg[0]);
+    for (uint64_t s = s_seg[1] + tid; s < s_seg[2]; s += kThreads) write_seg(s);
+  } else {
+    // Runs of equal keys: key at the head, value at the tail, index =
+    // inclusive head count - 1.
+    for (uint64_t i = tb + tid; i < te; i += kThreads) {
+      const uint32_t pos = (uint32_t)(i - tb);
+      const T yv = stage[pos];
+      const bool head = (s_bits[pos >> 5] >> (pos & 31)) & 1u;
+      if (head && p.out_keys)
+        st_raw_bits(p.out_keys, yv.heads - 1, p.out_key_esize, src_load_bits(p.keys, i));
+      const bool tail = (i + 1 == te) ? (s_head_te != 0)
+                                      : (((s_bits[(pos + 1) >> 5] >> ((pos + 1) & 31)) & 1u) != 0);
+      if (tail) {
+        st_cast<V>(p.out_dtype, p.out, yv.heads - 1, vop(p.init, yv.v));
+        if (i + 1 == n && p.count_dev) *p.count_dev = yv.heads;
+      }
+    }
+  }
+}
+
+template <class V>
+size_t seg_smem(int mode) {
+  return mode == kReduce ? sizeof(SegVal<V>) * SegCfg<V>::TILE : 0;
+}
+
+template <class V>
+int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_wide) {
+  using C = SegCfg<V>;
+  const uint64_t cap = in.len;
+  if (cap == 0) return MB_OK;
+  memcpy(&p.init, init_wide, sizeof(V));
+  const uint64_t tiles = (cap + C::TILE - 1) / C::TILE;
+  using T = SegVal<V>;
+  const size_t state_b = TileState<T, false>::bytes(tiles);
+  Scratch scratch;
+  MB_TRY(scratch.alloc(ex, 256 + state_b));
+  MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + state_b, ex->stream));
+  p.counter = scratch.as<uint32_t>();
+  p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
+  auto st = TileState<T, false>::make(scratch.as<char>() + 256, tiles);
+  const bool plain = src_plain(in, DTypeOf<V>::value) && (uintptr_t)in.data % 16 == 0 &&
+                     (p.mode == kReduce || (uintptr_t)p.out % 16 == 0);
+  const Src s = to_src(in);
+  const size_t smem = seg_smem<V>(p.mode);
+#define MB_SEG_LAUNCH(OPID)                                                                    \
+  do {                                                                                         \
+    if (plain) {                                                                               \
+      auto k = seg_kernel<V, OPID, true>;                                                      \
+      if (smem > 48 * 1024)                                                                    \
+        MB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      k<<<(unsigned)tiles, kThreads, smem, ex->stream>>>(s, cap, p, st);                       \
+    } else {                                                                                   \
+      auto k = seg_kernel<V, OPID, false>;                                                     \
+      if (smem > 48 * 1024)                                                                    \
+        MB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      k<<<(unsigned)tiles, kThreads, smem, ex->stream>>>(s, cap, p, st);                       \
+    }                                                                                          \
+  } while (0)
+  switch (p.op) {
+    case MB_OP_ADD: MB_SEG_LAUNCH(MB_OP_ADD); break;
+    case MB_OP_MIN: MB_SEG_LAUNCH(MB_OP_MIN); break;
+    case MB_OP_MAX: MB_SEG_LAUNCH(MB_OP_MAX); break;
+    default: MB_SEG_LAUNCH(kOpDyn); break;
+  }
+#undef MB_SEG_LAUNCH
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// Common set-up of every segmented call.  `out` holds per-element results
+// (scans) or per-segment / per-run results (reductions).
+int seg_entry(mb_executor* ex, const mb_src* values, int op, int mode, const void* init,
+              void* out, int out_dtype, const uint32_t* offsets, uint64_t nseg,
+              const mb_src* keys, void* out_keys, int out_key_esize, uint32_t* count_dev) {
+  const int ct = compute_type(values->vtype);
+  if (!op_valid_for(op, ct)) return set_error(MB_ERR_LAUNCH, "operator not defined for this type");
+  uint64_t init_wide = 0;
+  if (init) {
+    uint64_t raw = 0;
+    memcpy(&raw, init, dtype_size(values->vtype));
+    switch (values->vtype) {
+      case MB_I8: init_wide = (uint64_t)(int64_t)(int8_t)raw; break;
+      case MB_I16: init_wide = (uint64_t)(int64_t)(int16_t)raw; break;
+      default: init_wide = raw; break;
+    }
+  }
+#define MB_SEG_DISPATCH(V)                                          \
+  {                                                                 \
+    SegParams<V> p{};                                               \
+    p.op = op;                                                      \
+    p.mode = mode;                                                  \
+    p.heads_src = keys ? kHeadsKeys : kHeadsOffsets;                \
+    p.out_dtype = out_dtype;                                        \
+    p.offsets = offsets;                                            \
+    p.nseg = nseg;                                                  \
+    if (keys) p.keys = to_src(*keys);                               \
+    p.out = out;                                                    \
+    p.out_keys = out_keys;                                          \
+    p.out_key_esize = out_key_esize;                                \
+    p.count_dev = count_dev;                                        \
+    return seg_run<V>(ex, *values, p, &init_wide);                  \
+  }
+  switch (ct) {
+    case MB_U32: MB_SEG_DISPATCH(uint32_t)
+    case MB_I32: MB_SEG_DISPATCH(int32_t)
+    case MB_U64: MB_SEG_DISPATCH(uint64_t)
+    case MB_I64: MB_SEG_DISPATCH(int64_t)
+    case MB_F32: MB_SEG_DISPATCH(float)
+    case MB_F64: MB_SEG_DISPATCH(double)
+    default: break;
+  }
+#undef MB_SEG_DISPATCH
+  return set_error(MB_ERR_LAUNCH, "unsupported element type");
+}
+
+// ------------------------------------------------------ segmentation ----
+
+__global__ void validate_offsets_kernel(const uint32_t* off, uint64_t count, uint32_t* bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if ((i == 0 && off[0] != 0) || (i > 0 && off[i] < off[i - 1])) atomicMax(bad, 1u);
+  }
+}
+
+// offsets[0] = 0, offsets[s+1] = prefix[s]; flags a total above u32.
+__global__ void offsets_from_prefix_kernel(const uint64_t* prefix, uint64_t nseg, uint32_t* off,
+                                           uint32_t* status) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s <= nseg;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    if (s == 0) { off[0] = 0; continue; }
+    const uint64_t v = prefix[s - 1];
+    if (v > 0xFFFFFFFFull) atomicMax(status, 1u);
+    off[s] = (uint32_t)v;
+    if (s == nseg) status[1] = (uint32_t)v;
+  }
+}
+
+__global__ void segment_ids_kernel(const uint32_t* off, uint64_t nseg, uint32_t* ids, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    ids[i] = (uint32_t)(upper_bound_u32(off, nseg + 1, i) - 1);
+  }
+}
+
+unsigned grid_for_n(uint64_t n) {
+  uint64_t g = (n + 255) / 256;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 8));
+}
+
+int check_values_out(mb_executor* ex, const mb_src* values, const mb_col& out, uint64_t need) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, values, "values"));
+  MB_TRY(check_col(ex, out, "output"));
+  if (out.len < need)
+    return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", need, out.len);
+  if (compute_type(out.dtype) != compute_type(values->vtype))
+    return set_error(MB_ERR_LAUNCH, "output element type differs from the input's");
+  return MB_OK;
+}
+
+}  // namespace
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" {
+
+int mb_segmentation_validate_offsets(mb_executor* ex, const uint32_t* offsets,
+                                     uint64_t offset_count, uint32_t* value_count) {
+  MB_TRY(check_exec(ex));
+  if (offset_count == 0 || !offsets)
+    return set_error(MB_ERR_INVALID_SEGMENTATION, "segmentation is not a valid ordered partition");
+  MB_TRY(check_len_u32(offset_count - 1));
+  Scratch bad;
+  MB_TRY(bad.alloc(ex, 16));
+  MB_CUDA(cudaMemsetAsync(bad.ptr, 0, 16, ex->stream));
+  validate_offsets_kernel<<<grid_for_n(offset_count), 256, 0, ex->stream>>>(offsets, offset_count,
+                                                                           bad.as<uint32_t>());
+  MB_CUDA(cudaGetLastError());
+  MB_CUDA(cudaMemcpyAsync(bad.as<uint32_t>() + 1, offsets + offset_count - 1, 4,
+                          cudaMemcpyDeviceToDevice, ex->stream));
+  if (ex->capturing) return set_error(MB_ERR_LAUNCH, "validation cannot run inside graph capture");
+  MB_CUDA(cudaMemcpyAsync(ex->host_pinned, bad.ptr, 8, cudaMemcpyDeviceToHost, ex->stream));
+  MB_CUDA(cudaStreamSynchronize(ex->stream));
+  if (ex->host_pinned[0] != 0)
+    return set_error(MB_ERR_INVALID_SEGMENTATION, "segmentation is not a valid ordered partition");
+  if (value_count) *value_count = ex->host_pinned[1];
+  return MB_OK;
+}
+
+int mb_segmentation_from_lengths(mb_executor* ex, const mb_src* lengths, uint32_t* offsets,
+                                 uint32_t* value_count) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, lengths, "lengths"));
+  const uint64_t nseg = lengths->len;
+  if (nseg >= 0xFFFFFFFFull)
+    return set_error(MB_ERR_LENGTH_TOO_LARGE, "length does not fit in u32", nseg + 1);
+  Scratch pre, stat;
+  MB_TRY(stat.alloc(ex, 16));
+  MB_CUDA(cudaMemsetAsync(stat.ptr, 0, 16, ex->stream));
+  if (nseg > 0) {
+    MB_TRY(pre.alloc(ex, nseg * 8));
+    mb_src wide = *lengths;
+    wide.vtype = MB_U64;  // lengths summed in u64 to detect overflow
+    mb_col c{};
+    c.data = pre.ptr;
+    c.dtype = MB_U64;
+    c.len = nseg;
+    MB_TRY(mb_inclusive_scan(ex, &wide, MB_OP_ADD, c));
+  }
+  offsets_from_prefix_kernel<<<grid_for_n(nseg + 1), 256, 0, ex->stream>>>(
+      pre.as<uint64_t>(), nseg, offsets, stat.as<uint32_t>());
+  MB_CUDA(cudaGetLastError());
+  if (ex->capturing) return set_error(MB_ERR_LAUNCH, "validation cannot run inside graph capture");
+  MB_CUDA(cudaMemcpyAsync(ex->host_pinned, stat.ptr, 8, cudaMemcpyDeviceToHost, ex->stream));
+  MB_CUDA(cudaStreamSynchronize(ex->stream));
+  if (ex->host_pinned[0] != 0)
+    return set_error(MB_ERR_LENGTH_TOO_LARGE, "length does not fit in u32", 0x100000000ull);
+  if (value_count) *value_count = ex->host_pinned[1];
+  return MB_OK;
+}
+
+int mb_segmentation_segment_ids(mb_executor* ex, const uint32_t* offsets, uint64_t segment_count,
+                                uint32_t* ids, uint64_t value_count) {
+  MB_TRY(check_exec(ex));
+  if (value_count == 0) return MB_OK;
+  segment_ids_kernel<<<grid_for_n(value_count), 256, 0, ex->stream>>>(offsets, segment_count, ids,
+                                                                     value_count);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int mb_seg_inclusive_scan(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
+                          uint64_t segment_count, int op, mb_col out) {
+  MB_TRY(check_values_out(ex, values, out, values ? values->len : 0));
+  return seg_entry(ex, values, op, kScanIncl, nullptr, out.data, out.dtype, offsets,
+                   segment_count, nullptr, nullptr, 0, nullptr);
+}
+
+int mb_seg_exclusive_scan(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
+                          uint64_t segment_count, int op, const void* init, mb_col out) {
+  MB_TRY(check_values_out(ex, values, out, values ? values->len : 0));
+  if (!init) return set_error(MB_ERR_LAUNCH, "exclusive scan needs an init value");
+  return seg_entry(ex, values, op, kScanExcl, init, out.data, out.dtype, offsets, segment_count,
+                   nullptr, nullptr, 0, nullptr);
+}
+
+int mb_seg_reduce(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
+                  uint64_t segment_count, int op, const void* init, mb_col out) {
+  MB_TRY(check_values_out(ex, values, out, segment_count));
+  if (!init) return set_error(MB_ERR_LAUNCH, "reduce needs an init value");
+  if (!op_commutative(op) && op != MB_OP_TAKE_RIGHT && op != MB_OP_TAKE_LEFT)
+    return set_error(MB_ERR_LAUNCH, "operator not supported");
+  if (values->len == 0) return segment_count ? mb_fill(ex, init, out) : MB_OK;
+  return seg_entry(ex, values, op, kReduce, init, out.data, out.dtype, offsets, segment_count,
+                   nullptr, nullptr, 0, nullptr);
+}
+
+int mb_inclusive_scan_by_key(mb_executor* ex, const mb_src* keys, int key_eq,
+                             const mb_src* values, int op, mb_col out) {
+  MB_TRY(check_values_out(ex, values, out, values ? values->len : 0));
+  MB_TRY(check_src(ex, keys, "keys"));
+  if (key_eq != MB_EQUAL) return set_error(MB_ERR_LAUNCH, "by-key algorithms take EQUAL");
+  if (keys->len != values->len)
+    return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", keys->len, values->len);
+  return seg_entry(ex, values, op, kScanIncl, nullptr, out.data, out.dtype, nullptr, 0, keys,
+                   nullptr, 0, nullptr);
+}
+
+int mb_exclusive_scan_by_key(mb_executor* ex, const mb_src* keys, int key_eq,
+                             const mb_src* values, int op, const void* init, mb_col out) {
+  MB_TRY(check_values_out(ex, values, out, values ? values->len : 0));
+  MB_TRY(check_src(ex, keys, "keys"));
+  if (key_eq != MB_EQUAL) return set_error(MB_ERR_LAUNCH, "by-key algorithms take EQUAL");
+  if (keys->len != values->len)
+    return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", keys->len, values->len);
+  if (!init) return set_error(MB_ERR_LAUNCH, "exclusive scan needs an init value");
+  return seg_entry(ex, values, op, kScanExcl, init, out.data, out.dtype, nullptr, 0, keys,
+                   nullptr, 0, nullptr);
+}
+
+int mb_reduce_by_key(mb_executor* ex, const mb_src* keys, int key_eq, const mb_src* values,
+                     int nvals, const int* ops, const uint64_t* inits, mb_col out_keys,
+                     const mb_col* out_values, uint32_t* count_dev, uint32_t* count_host) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, keys, "keys"));
+  MB_TRY(check_col(ex, out_keys, "key output"));
+  if (key_eq != MB_EQUAL) return set_error(MB_ERR_LAUNCH, "by-key algorithms take EQUAL");
+  if (nvals < 1 || nvals > 12) return set_error(MB_ERR_LAUNCH, "values take 1 to 12 columns");
+  const uint64_t n = keys->len;
+  if (dtype_size(out_keys.dtype) != dtype_size(keys->vtype))
+    return set_error(MB_ERR_LAUNCH, "key output element type differs");
+  for (int c = 0; c < nvals; ++c) {
+    if (values[c].len != n)
+      return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", n, values[c].len);
+    MB_TRY(check_values_out(ex, &values[c], out_values[c], 0));
+  }
+  Scratch cnt;
+  if (!count_dev) {
+    MB_TRY(cnt.alloc(ex, 16));
+    count_dev = cnt.as<uint32_t>();
+  }
+  if (n == 0) {
+    MB_CUDA(cudaMemsetAsync(count_dev, 0, 4, ex->stream));
+  } else {
+    for (int c = 0; c < nvals; ++c) {
+      MB_TRY(seg_entry(ex, &values[c], ops[c], kReduce, &inits[c], out_values[c].data,
+                       out_values[c].dtype, nullptr, 0, keys, c == 0 ? out_keys.data : nullptr,
+                       (int)dtype_size(out_keys.dtype), c == 0 ? count_dev : nullptr));
+    }
+  }
+  if (count_host) MB_TRY(read_u32(ex, count_dev, count_host));
+  return MB_OK;
+}
+
+}  // extern "C"

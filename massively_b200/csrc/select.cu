@@ -45,7 +45,7 @@ struct SelParams {
   uint32_t* count_dev;
   const uint32_t* boundary_dev;  // partition: number of kept rows
   uint32_t* counter;
-  uint32_t* status;
+  DevErr err;
 };
 
 __device__ __forceinline__ void st_raw(void* p, uint64_t i, int esize, uint64_t bits) {
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
     } else {
       if (lane == 0) st.publish(tile, kFlagAgg, agg);
       excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add,
-                                                                           p.status, 0u);
+                                                                           p.err, 0u);
       if (lane == 0) st.publish(tile, kFlagIncl, excl + agg);
     }
     if (lane == 0) {
@@ -205,7 +205,7 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
     MB_TRY(scratch.alloc(ex, 256 + tiles * 8));
     MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + tiles * 8, ex->stream));
     p.counter = scratch.as<uint32_t>();
-    p.status = ex->status_dev;
+    p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
     auto st = TileState<uint32_t, true>::make(scratch.as<char>() + 256, tiles);
     if (fast)
       select_kernel<true><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);

@@ -241,6 +241,44 @@ int mb_sort(mb_executor* ex, const mb_src* keys, int less, mb_col out) {
   return sort_general(ex, keys, 1, &ieee, &desc, nullptr, 0, nullptr, &out);
 }
 
+// ForEachSegment(Sort(less)) (massively/src/seg/mod.rs:379-425): a stable
+// order of (segment id, value) pairs -- the segment id primary -- sorts every
+// segment in place of massively's two global comparison sorts and three
+// permutation applications.  Segment ids need ceil(log2(segments)/8) digit
+// passes; constant high digits are skipped by the onesweep plan.
+int mb_seg_sort(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
+                uint64_t segment_count, int less, mb_col out) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, values, "values"));
+  MB_TRY(check_col(ex, out, "output"));
+  const uint64_t n = values->len;
+  if (out.len < n) return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", n, out.len);
+  if (less < MB_LESS || less > MB_TOTAL_LESS)
+    return set_error(MB_ERR_LAUNCH, "seg sort takes LESS, GREATER or TOTAL_LESS");
+  if (n == 0) return MB_OK;
+  Scratch ids, ids_out;
+  MB_TRY(ids.alloc(ex, n * 4));
+  MB_TRY(ids_out.alloc(ex, n * 4));
+  MB_TRY(mb_segmentation_segment_ids(ex, offsets, segment_count, ids.as<uint32_t>(), n));
+  mb_src keys[2];
+  keys[0] = mb_src{};
+  keys[0].kind = MB_SRC_COLUMN;
+  keys[0].dtype = keys[0].vtype = MB_U32;
+  keys[0].map = MB_UN_IDENTITY;
+  keys[0].data = ids.ptr;
+  keys[0].len = n;
+  keys[1] = *values;
+  int ieee[2] = {0, 0}, desc[2] = {0, 0};
+  comparator_mode(less, values->vtype, &ieee[1], &desc[1]);
+  mb_col outs[2];
+  outs[0] = mb_col{};
+  outs[0].data = ids_out.ptr;
+  outs[0].dtype = MB_U32;
+  outs[0].len = n;
+  outs[1] = out;
+  return sort_general(ex, keys, 2, ieee, desc, nullptr, 0, nullptr, outs);
+}
+
 int mb_sort_by_key(mb_executor* ex, const mb_src* keys, int less, const mb_src* values, int nvals,
                    const mb_col* out_keys, const mb_col* out_values) {
   MB_TRY(check_exec(ex));

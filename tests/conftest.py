@@ -12,6 +12,17 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
+@pytest.fixture(autouse=True)
+def _device_errors_checked(request):
+    """After every test that used an executor `ex`, synchronise it so a
+    device-side failure (bounded look-back expiry, bounds check) is reported
+    by the test that caused it."""
+    yield
+    ex = getattr(request.node, "funcargs", {}).get("ex")
+    if ex is not None and hasattr(ex, "sync"):
+        ex.sync()
+
+
 @pytest.fixture(scope="session")
 def orc():
     from oracle import oracle
