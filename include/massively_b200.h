@@ -130,6 +130,9 @@ typedef enum mb_pred2 {
  *   REVERSE      data[len - 1 - i]
  *   REPEAT_EACH  data[i / a]
  *   TILE         data[i % a]
+ *   ADJACENT     i == 0 ? data[0] : op(data[i-1], data[i]), op = mb_op id in
+ *                `b` (lazy::adjacent_difference, massively/src/api/lazy.rs:
+ *                869-902); `map` must be MB_UN_IDENTITY
  * and then applies `map` (mb_unary), converting to `vtype`. */
 typedef enum mb_src_kind {
   MB_SRC_COLUMN = 0,
@@ -139,7 +142,8 @@ typedef enum mb_src_kind {
   MB_SRC_PERMUTE = 4,
   MB_SRC_REVERSE = 5,
   MB_SRC_REPEAT_EACH = 6,
-  MB_SRC_TILE = 7
+  MB_SRC_TILE = 7,
+  MB_SRC_ADJACENT = 8
 } mb_src_kind;
 
 typedef struct mb_src {
@@ -328,6 +332,16 @@ int mb_segmentation_from_lengths(mb_executor* exec, const mb_src* lengths, uint3
 /* Segmentation::segment_ids (flat value -> segment index). */
 int mb_segmentation_segment_ids(mb_executor* exec, const uint32_t* offsets,
                                 uint64_t segment_count, uint32_t* ids, uint64_t value_count);
+/* Segmentation::lengths and local_indices (segmentation.rs:346-411). */
+int mb_segmentation_lengths(mb_executor* exec, const uint32_t* offsets, uint64_t segment_count,
+                            uint32_t* lengths);
+int mb_segmentation_local_indices(mb_executor* exec, const uint32_t* offsets,
+                                  uint64_t segment_count, uint32_t* local, uint64_t value_count);
+/* Segmentation::from_segment_ids (segmentation.rs:290-335): ids must be
+ * non-decreasing and below segment_count; offsets[s] = lower_bound(ids, s)
+ * for s = 0..segment_count (segment_count + 1 entries, one synchronisation). */
+int mb_segmentation_from_segment_ids(mb_executor* exec, const mb_src* ids, uint64_t segment_count,
+                                     uint32_t* offsets);
 
 /* ForEachSegment(InclusiveScan(op)) / ExclusiveScan(op, init)
  * (massively/src/seg/mod.rs:525-572). */
@@ -368,7 +382,7 @@ int mb_graph_destroy(mb_graph* graph);
 
 /* Selects the kernel configuration (tile shape) used by an algorithm family
  * for later calls on `exec`; -1 restores the built-in default.  `family` is
- * one of the MB_TUNE_* ids; `config` indexes mb_tune_configs(). */
+ * one of the MB_TUNE_* ids; `config` is below mb_tune_config_count(family). */
 enum { MB_TUNE_SCAN = 0, MB_TUNE_RADIX = 1, MB_TUNE_REDUCE = 2, MB_TUNE_SELECT = 3 };
 int mb_tune_config_count(int family);
 int mb_tune_set(mb_executor* exec, int family, int config);

@@ -18,7 +18,7 @@ U8, U16, U32, U64, I8, I16, I32, I64, F32, F64 = range(10)
 OK, LENGTH_MISMATCH, OUTPUT_TOO_SHORT, LENGTH_TOO_LARGE, INVALID_SEGMENTATION, \
     UNBOUND_COLUMN, FOREIGN_EXECUTOR, LAUNCH = range(8)
 SRC_COLUMN, SRC_CONSTANT, SRC_COUNTING, SRC_STRIDE, SRC_PERMUTE, SRC_REVERSE, \
-    SRC_REPEAT_EACH, SRC_TILE = range(8)
+    SRC_REPEAT_EACH, SRC_TILE, SRC_ADJACENT = range(9)
 
 
 class mb_src(C.Structure):
@@ -87,6 +87,9 @@ def _declare(L: C.CDLL) -> None:
         "mb_segmentation_validate_offsets": (i32, [vp, vp, u64, pu32]),
         "mb_segmentation_from_lengths": (i32, [vp, src, vp, pu32]),
         "mb_segmentation_segment_ids": (i32, [vp, vp, u64, vp, u64]),
+        "mb_segmentation_lengths": (i32, [vp, vp, u64, vp]),
+        "mb_segmentation_local_indices": (i32, [vp, vp, u64, vp, u64]),
+        "mb_segmentation_from_segment_ids": (i32, [vp, src, u64, vp]),
         "mb_seg_inclusive_scan": (i32, [vp, src, vp, u64, i32, col]),
         "mb_seg_exclusive_scan": (i32, [vp, src, vp, u64, i32, vp, col]),
         "mb_seg_reduce": (i32, [vp, src, vp, u64, i32, vp, col]),

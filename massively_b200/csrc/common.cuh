@@ -173,6 +173,14 @@ __device__ __forceinline__ int64_t sext_bits(int dtype, uint64_t bits) {
 // and converts the result to T (the consumer's compute type).
 template <class T>
 __device__ __forceinline__ T map_to(int map, int dtype, uint64_t bits) {
+  // Identity loads of the same floating type keep their exact bits (NaN
+  // payloads included).
+  if constexpr (std::is_same<T, float>::value) {
+    if (map == MB_UN_IDENTITY && dtype == MB_F32) return __uint_as_float((uint32_t)bits);
+  }
+  if constexpr (std::is_same<T, double>::value) {
+    if (map == MB_UN_IDENTITY && dtype == MB_F64) return __longlong_as_double((long long)bits);
+  }
   if (dtype == MB_F32 || dtype == MB_F64) {
     double x = dtype == MB_F32 ? (double)__uint_as_float((uint32_t)bits)
                                : __longlong_as_double((long long)bits);
@@ -226,6 +234,12 @@ __device__ __forceinline__ T map_to(int map, int dtype, uint64_t bits) {
 template <class T>
 __device__ __forceinline__ T src_load(const Src& s, uint64_t i) {
   uint64_t bits;
+  if (s.kind == MB_SRC_ADJACENT) {
+    const T cur = map_to<T>(MB_UN_IDENTITY, s.dtype, ld_bits(s.dtype, s.data, i));
+    if (i == 0) return cur;
+    const T prev = map_to<T>(MB_UN_IDENTITY, s.dtype, ld_bits(s.dtype, s.data, i - 1));
+    return op_apply_rt<T>((int)s.b, prev, cur);
+  }
   switch (s.kind) {
     case MB_SRC_COLUMN: bits = ld_bits(s.dtype, s.data, i); break;
     case MB_SRC_CONSTANT: bits = s.a; break;
@@ -411,6 +425,22 @@ int read_u32(mb_executor* ex, const uint32_t* dev, uint32_t* host);
 }  // namespace mb
 
 namespace mb {
+
+// The same encodings on raw unsigned bits (U = uint32_t / uint64_t), so keys
+// never pass through floating-point registers.
+enum KeyEnc : int { kEncUnsigned = 0, kEncSigned = 1, kEncFloat = 2 };
+
+template <class U, int ENC>
+__device__ __forceinline__ U enc_bits(U raw) {
+  constexpr U sign = (U)1 << (sizeof(U) * 8 - 1);
+  if constexpr (ENC == kEncFloat) {
+    return (raw & sign) ? (U)~raw : (U)(raw ^ sign);
+  } else if constexpr (ENC == kEncSigned) {
+    return (U)(raw ^ sign);
+  } else {
+    return raw;
+  }
+}
 
 // Order-preserving radix encoding of massively/src/core/radix.rs:46-89:
 // unsigned as is, signed with the sign bit flipped, floats in total order

@@ -14,12 +14,13 @@
 //                  in the output -- on the device, so nothing synchronises and
 //                  the whole sort can be captured in a CUDA graph;
 //   3. onesweep:   per active digit, one kernel: every tile ranks its keys
-//                  stably (warp match on the digit, per-warp counters in
-//                  shared memory), publishes its 256 digit counts, obtains the
-//                  counts of all earlier tiles by a per-digit decoupled
-//                  look-back, and scatters keys (then values) through a
-//                  shared-memory staging buffer so consecutive threads write
-//                  consecutive addresses of each digit run.
+//                  stably (warp match on the digit, per-warp counters bumped
+//                  with shared-memory atomics), publishes its 256 digit
+//                  counts, stages its keys in tile-sorted order in shared
+//                  memory, obtains the counts of all earlier tiles by a
+//                  per-digit decoupled look-back (overlapped with the value
+//                  loads), and writes keys and values so consecutive threads
+//                  store consecutive addresses of each digit run.
 //
 // Keys are ordered by massively's radix encodings (massively/src/core/
 // radix.rs:46-89): unsigned as is, signed with the sign bit flipped, floats
@@ -41,9 +42,12 @@ constexpr int kBins = 1 << kRadixBits;
 constexpr int kHistThreads = 256;
 constexpr uint32_t kCountMask = 0x3FFFFFFFu;  // status: 2 flag bits + 30 count bits
 
-template <class K>
+// Keys travel as their raw unsigned bits (K = uint32_t / uint64_t) and are
+// never held in floating-point registers; ENC (enc_bits, common.cuh) selects
+// massively's encoding of the element type they came from.
+template <class K, int ENC>
 __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
-  return (uint32_t)((radix_enc<K>(k) >> shift) & (kBins - 1));
+  return (uint32_t)((enc_bits<K, ENC>(k) >> shift) & (kBins - 1));
 }
 
 // Buffer plan of one sort, filled on the device by the plan kernel.
@@ -59,7 +63,7 @@ struct PassPlan {
 
 // ----------------------------------------------------------- histogram --
 
-template <class K, int PASSES>
+template <class K, int ENC, int PASSES>
 __global__ void __launch_bounds__(kHistThreads)
     radix_histogram_kernel(const K* __restrict__ keys, uint64_t n, uint32_t* __restrict__ hist) {
   __shared__ uint32_t sh[PASSES][kBins];
@@ -69,7 +73,7 @@ __global__ void __launch_bounds__(kHistThreads)
   for (uint64_t i = blockIdx.x * (uint64_t)kHistThreads + threadIdx.x; i - threadIdx.x < n;
        i += step) {
     const bool valid = i < n;
-    const auto u = valid ? radix_enc<K>(keys[i]) : (typename UnsignedOf<K>::type)0;
+    const K u = valid ? enc_bits<K, ENC>(__ldcs(keys + i)) : (K)0;
 #pragma unroll
     for (int p = 0; p < PASSES; ++p) {
       const uint32_t d = (uint32_t)((u >> (p * kRadixBits)) & (kBins - 1));
@@ -108,7 +112,6 @@ __global__ void __launch_bounds__(kBins)
     if ((uint64_t)c == n) s_trivial[p] = 1;
     s_scan[d] = c;
     __syncthreads();
-    // Hillis-Steele inclusive scan over 256 bins.
     for (int off = 1; off < kBins; off <<= 1) {
       uint32_t v = d >= off ? s_scan[d - off] : 0;
       __syncthreads();
@@ -131,7 +134,8 @@ __global__ void __launch_bounds__(kBins)
         continue;
       }
       ++i;
-      // X_i is the output when (m - i) is even, else the temporary.
+      // The i-th active pass writes the output when (m - i) is even, else
+      // the temporary, so the last active pass lands in the output.
       const bool to_out = ((m - i) % 2) == 0;
       void* nk = to_out ? out_k : tmp_k;
       void* nv = to_out ? out_v : tmp_v;
@@ -162,14 +166,15 @@ struct OnesweepSmem {
   uint32_t warp_cnt[WARPS][kBins];  // per-warp digit counts, then exclusive prefixes
   uint32_t tile_start[kBins];       // exclusive prefix of the tile's digit counts
   uint32_t delta[kBins];            // global base - tile start, per digit
+  uint32_t wsum[kBins / 32];        // digit-scan warp totals
   uint32_t tile_id;
   K keys[TILE];
   V vals[std::is_same<V, uint8_t>::value ? 1 : TILE];
 };
 
 // V = uint8_t means "keys only".
-template <class K, class V, int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS)
+template <class K, int ENC, class V, int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
     radix_onesweep_kernel(const PassPlan* __restrict__ plan, int pass, uint64_t n,
                           const uint32_t* __restrict__ digit_offsets, uint32_t* __restrict__ status,
                           uint32_t* __restrict__ counter, DevErr err) {
@@ -193,7 +198,7 @@ __global__ void __launch_bounds__(THREADS)
     V* ov = (V*)plan->out_v[0];
     for (uint64_t i = blockIdx.x * (uint64_t)THREADS + tid; i < n;
          i += (uint64_t)gridDim.x * THREADS) {
-      if (ok) ok[i] = ik[i];
+      ok[i] = ik[i];
       if constexpr (!KEYS_ONLY) ov[i] = iv[i];
     }
     return;
@@ -215,18 +220,73 @@ __global__ void __launch_bounds__(THREADS)
   // Warp-striped loads: item k of lane l is at warp_base + k*32 + l, so the
   // rounds below visit the keys in input order (stability).
   K key[ITEMS];
-  uint32_t dig[ITEMS];
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
     const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
-    if (i < n) {
-      key[k] = __ldcs(in_k + i);
-      dig[k] = digit_of<K>(key[k], shift);
-    } else {
-      key[k] = K(0);
-      dig[k] = kBins;  // out-of-range digit: never counted or written
+    key[k] = i < n ? __ldcs(in_k + i) : K(0);
+  }
+  auto digit_k = [&](int k) -> uint32_t {
+    const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+    return i < n ? digit_of<K, ENC>(key[k], shift) : (uint32_t)kBins;  // kBins: never counted
+  };
+
+  // Stable rank within the warp: peers with the same digit in a round are
+  // ordered by lane; rounds are in input order.  The leader's atomic add on
+  // the warp's digit counter returns the count of earlier rounds; a warp
+  // issues its atomics in program order, so rounds apply in order.
+  uint32_t rank[ITEMS];
+  const unsigned lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t d = digit_k(k);
+    const unsigned peers = __match_any_sync(kFull, d);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader && d < kBins) base = atomicAdd(&sm.warp_cnt[warp][d], (uint32_t)__popc(peers));
+    rank[k] = __shfl_sync(kFull, base, leader) + __popc(peers & lt_mask);
+  }
+  __syncthreads();
+
+  // Per digit (thread d): exclusive prefix over warps and the tile count,
+  // published at once; then the tile-local exclusive scan over digits.
+  uint32_t tile_count = 0;
+  if (tid < kBins) {
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+      const uint32_t c = sm.warp_cnt[w][tid];
+      sm.warp_cnt[w][tid] = tile_count;
+      tile_count += c;
+    }
+    const uint32_t flag = tile == 0 ? kFlagIncl : kFlagAgg;
+    st_relaxed_u32(status + tile * kBins + tid, (flag << 30) | tile_count);
+    uint32_t incl = tile_count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, incl, off);
+      if (lane >= off) incl += o;
+    }
+    if (lane == 31) sm.wsum[warp] = incl;
+    sm.tile_start[tid] = incl - tile_count;  // warp-local exclusive
+  }
+  __syncthreads();
+  if (tid < kBins) {
+    uint32_t add = 0;
+    for (int w = 0; w < warp; ++w) add += sm.wsum[w];
+    sm.tile_start[tid] += add;
+  }
+  __syncthreads();
+
+  // Stage keys at their tile-sorted positions; keep the positions.
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t d = digit_k(k);
+    if (d < kBins) {
+      const uint32_t pos = sm.tile_start[d] + sm.warp_cnt[warp][d] + rank[k];
+      rank[k] = pos;
+      sm.keys[pos] = key[k];
     }
   }
+  // Value loads go out before the look-back so their latency overlaps it.
   V val[KEYS_ONLY ? 1 : ITEMS];
   if constexpr (!KEYS_ONLY) {
 #pragma unroll
@@ -236,59 +296,10 @@ __global__ void __launch_bounds__(THREADS)
     }
   }
 
-  // Stable rank within the warp: peers with the same digit in a round are
-  // ordered by lane; rounds are in input order.
-  uint32_t rank[ITEMS];
-  const unsigned lt_mask = (1u << lane) - 1u;
-#pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t d = dig[k];
-    const unsigned peers = __match_any_sync(kFull, d);
-    const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if (lane == leader && d < kBins) {
-      base = sm.warp_cnt[warp][d];
-      sm.warp_cnt[warp][d] = base + __popc(peers);
-    }
-    base = __shfl_sync(kFull, base, leader);
-    rank[k] = base + __popc(peers & lt_mask);
-    __syncwarp();  // order this round's counter update before the next round's read
-  }
-  __syncthreads();
-
-  // Per digit (thread d): exclusive prefix over warps, tile count.
-  uint32_t tile_count = 0;
-  if (tid < kBins) {
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) {
-      const uint32_t c = sm.warp_cnt[w][tid];
-      sm.warp_cnt[w][tid] = tile_count;
-      tile_count += c;
-    }
-    // Publish this tile's count for digit `tid`.
-    uint32_t* row = status + tile * kBins;
-    const uint32_t flag = tile == 0 ? kFlagIncl : kFlagAgg;
-    st_relaxed_u32(row + tid, (flag << 30) | tile_count);
-  }
-  // Tile-local exclusive scan of the digit counts (block scan over 256).
-  if (tid < kBins) sm.tile_start[tid] = tile_count;
-  __syncthreads();
-  for (int off = 1; off < kBins; off <<= 1) {
-    uint32_t v = 0;
-    if (tid < kBins && tid >= off) v = sm.tile_start[tid - off];
-    __syncthreads();
-    if (tid < kBins) sm.tile_start[tid] += v;
-    __syncthreads();
-  }
-  if (tid < kBins) sm.tile_start[tid] -= tile_count;
-
-  // Decoupled look-back, one digit per thread.
+  // Decoupled look-back, one digit per thread, eight predecessors per step.
   if (tid < kBins) {
     uint32_t excl = 0;
     if (tile > 0) {
-      // Eight predecessors per step, loaded independently, then folded in
-      // order until the first inclusive count (or an unpublished tile, which
-      // is polled again).
       constexpr int kBatch = 8;
       SpinGuard guard(err.abort);
       int64_t t = (int64_t)tile - 1;  // next predecessor to account for
@@ -313,30 +324,26 @@ __global__ void __launch_bounds__(THREADS)
         if (!done && used < kBatch && guard.expired()) { failed = true; break; }
       }
       if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-      st_relaxed_u32(status + tile * kBins + tid, (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
+      st_relaxed_u32(status + tile * kBins + tid,
+                     (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
     }
     sm.delta[tid] = digit_offsets[pass * kBins + tid] + excl - sm.tile_start[tid];
   }
-  __syncthreads();
-
-  // Stage keys in shared memory in tile-sorted order.
+  if constexpr (!KEYS_ONLY) {
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t d = dig[k];
-    if (d < kBins) {
-      const uint32_t pos = sm.tile_start[d] + sm.warp_cnt[warp][d] + rank[k];
-      rank[k] = pos;
-      sm.keys[pos] = key[k];
-      if constexpr (!KEYS_ONLY) sm.vals[pos] = val[k];
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
+      if (i < n) sm.vals[rank[k]] = val[k];
     }
   }
   __syncthreads();
+
   const uint64_t valid = n - tile_base < (uint64_t)TILE ? n - tile_base : (uint64_t)TILE;
   // Coalesced write-out: position i of the sorted tile goes to delta[d] + i.
 #pragma unroll 4
   for (int i = tid; i < (int)valid; i += THREADS) {
     const K kk = sm.keys[i];
-    const uint32_t d = digit_of<K>(kk, shift);
+    const uint32_t d = digit_of<K, ENC>(kk, shift);
     const uint32_t o = sm.delta[d] + (uint32_t)i;
     if (o >= n) {  // only reachable after a failed look-back
       raise_device_error(err, MB_DEV_ERR_BOUNDS);
@@ -364,7 +371,7 @@ constexpr RadixCfg kRadixCfgs[] = {
 };
 constexpr int kRadixDefault = 0;
 
-template <class K, class V, int THREADS, int ITEMS>
+template <class K, int ENC, class V, int THREADS, int ITEMS>
 int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v,
                       uint64_t n) {
   constexpr int PASSES = (int)sizeof(K);
@@ -373,8 +380,8 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   const uint64_t tiles = (n + TILE - 1) / TILE;
   if (n >= (1ull << 30))
     return set_error(MB_ERR_LENGTH_TOO_LARGE, "radix sort supports fewer than 2^30 items", n);
-  // Scratch: [plan][hist P*256][counters P (padded)][status P*tiles*256]
-  // [tmp keys][tmp values]
+  // Scratch: [plan][hist P*256][counters + abort word][status P*tiles*256]
+  // [tmp keys][tmp values][keys output when none is given]
   const size_t plan_b = ((sizeof(PassPlan) + 255) / 256) * 256;
   const size_t hist_b = (size_t)PASSES * kBins * 4;
   const size_t cnt_b = 256;
@@ -398,46 +405,47 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ex->device);
   const uint64_t hist_blocks = std::min<uint64_t>((n + kHistThreads * 16 - 1) / (kHistThreads * 16),
                                                   (uint64_t)sms * 4);
-  radix_histogram_kernel<K, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks), kHistThreads,
+  radix_histogram_kernel<K, ENC, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks), kHistThreads,
                                       0, ex->stream>>>(in_k, n, hist);
   MB_CUDA(cudaGetLastError());
   radix_plan_kernel<<<1, kBins, 0, ex->stream>>>(hist, PASSES, n, plan, in_k, final_k, tmp_k,
                                                  in_v, out_v, tmp_v);
   MB_CUDA(cudaGetLastError());
   const size_t smem = onesweep_smem<K, V, THREADS, ITEMS>();
-  auto kern = radix_onesweep_kernel<K, V, THREADS, ITEMS>;
+  auto kern = radix_onesweep_kernel<K, ENC, V, THREADS, ITEMS>;
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const DevErr err{ex->status_dev, counters + 32};
   for (int p = 0; p < PASSES; ++p) {
-    kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(plan, p, n, hist, status + (size_t)p * tiles * kBins,
-                                                         counters + p,
-                                                         DevErr{ex->status_dev, counters + 32});
+    kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
+        plan, p, n, hist, status + (size_t)p * tiles * kBins, counters + p, err);
     MB_CUDA(cudaGetLastError());
   }
   return MB_OK;
 }
 
-template <class K, class V>
+template <class K, int ENC, class V>
 int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v, uint64_t n) {
   if (n == 0) return MB_OK;
   int cfg = ex->tune[MB_TUNE_RADIX];
   if (cfg < 0) cfg = kRadixDefault;
   switch (cfg) {
-    case 1: return onesweep_sort_cfg<K, V, 256, 24>(ex, in_k, in_v, out_k, out_v, n);
-    case 2: return onesweep_sort_cfg<K, V, 512, 16>(ex, in_k, in_v, out_k, out_v, n);
-    default: return onesweep_sort_cfg<K, V, 256, 16>(ex, in_k, in_v, out_k, out_v, n);
+    case 1: return onesweep_sort_cfg<K, ENC, V, 256, 24>(ex, in_k, in_v, out_k, out_v, n);
+    case 2: return onesweep_sort_cfg<K, ENC, V, 512, 16>(ex, in_k, in_v, out_k, out_v, n);
+    default: return onesweep_sort_cfg<K, ENC, V, 256, 16>(ex, in_k, in_v, out_k, out_v, n);
   }
 }
 
-// Dispatch on the key type and the value width (0 = keys only, 4, 8).
-template <class K>
+// Dispatch on the value width (0 = keys only, 4, 8).  K is the unsigned
+// integer type of the key's width, ENC its element type's encoding.
+template <class K, int ENC>
 int sort_keys_vals(mb_executor* ex, const void* ik, const void* iv, void* ok, void* ov,
                    size_t vsize, uint64_t n) {
   switch (vsize) {
-    case 0: return onesweep_sort<K, uint8_t>(ex, (const K*)ik, nullptr, (K*)ok, nullptr, n);
-    case 4: return onesweep_sort<K, uint32_t>(ex, (const K*)ik, (const uint32_t*)iv, (K*)ok,
-                                              (uint32_t*)ov, n);
-    case 8: return onesweep_sort<K, uint64_t>(ex, (const K*)ik, (const uint64_t*)iv, (K*)ok,
-                                              (uint64_t*)ov, n);
+    case 0: return onesweep_sort<K, ENC, uint8_t>(ex, (const K*)ik, nullptr, (K*)ok, nullptr, n);
+    case 4: return onesweep_sort<K, ENC, uint32_t>(ex, (const K*)ik, (const uint32_t*)iv, (K*)ok,
+                                                   (uint32_t*)ov, n);
+    case 8: return onesweep_sort<K, ENC, uint64_t>(ex, (const K*)ik, (const uint64_t*)iv, (K*)ok,
+                                                   (uint64_t*)ov, n);
     default: return set_error(MB_ERR_LAUNCH, "radix values must be 4 or 8 bytes wide");
   }
 }
@@ -449,12 +457,12 @@ int sort_keys_vals(mb_executor* ex, const void* ik, const void* iv, void* ok, vo
 int radix_sort_plain(mb_executor* ex, int kdt, const void* ik, const void* iv, void* ok, void* ov,
                      size_t vsize, uint64_t n) {
   switch (kdt) {
-    case MB_U32: return sort_keys_vals<uint32_t>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_I32: return sort_keys_vals<int32_t>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_F32: return sort_keys_vals<float>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_U64: return sort_keys_vals<uint64_t>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_I64: return sort_keys_vals<int64_t>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_F64: return sort_keys_vals<double>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_U32: return sort_keys_vals<uint32_t, kEncUnsigned>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_I32: return sort_keys_vals<uint32_t, kEncSigned>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_F32: return sort_keys_vals<uint32_t, kEncFloat>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_U64: return sort_keys_vals<uint64_t, kEncUnsigned>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_I64: return sort_keys_vals<uint64_t, kEncSigned>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_F64: return sort_keys_vals<uint64_t, kEncFloat>(ex, ik, iv, ok, ov, vsize, n);
     default: return set_error(MB_ERR_LAUNCH, "radix keys must be 32- or 64-bit elements");
   }
 }

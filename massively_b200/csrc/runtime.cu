@@ -65,11 +65,14 @@ int check_src(mb_executor* ex, const mb_src* s, const char* what) {
     return set_error(MB_ERR_FOREIGN_EXECUTOR, "executor does not own this device data");
   if (!dtype_valid(s->dtype) || !dtype_valid(s->vtype))
     return set_error(MB_ERR_LAUNCH, std::string(what) + ": unknown element type");
-  if (s->kind < MB_SRC_COLUMN || s->kind > MB_SRC_TILE)
+  if (s->kind < MB_SRC_COLUMN || s->kind > MB_SRC_ADJACENT)
     return set_error(MB_ERR_LAUNCH, std::string(what) + ": unknown view kind");
+  if (s->kind == MB_SRC_ADJACENT &&
+      (s->map != MB_UN_IDENTITY || !op_valid_for((int)s->b, compute_type(s->vtype))))
+    return set_error(MB_ERR_LAUNCH, std::string(what) + ": bad adjacent view");
   bool needs_data = s->kind == MB_SRC_COLUMN || s->kind == MB_SRC_PERMUTE ||
                     s->kind == MB_SRC_REVERSE || s->kind == MB_SRC_REPEAT_EACH ||
-                    s->kind == MB_SRC_TILE;
+                    s->kind == MB_SRC_TILE || s->kind == MB_SRC_ADJACENT;
   if (needs_data && s->data == nullptr && s->len > 0)
     return set_error(MB_ERR_UNBOUND_COLUMN, "column is not bound to device storage");
   if (s->kind == MB_SRC_PERMUTE && s->index == nullptr && s->len > 0)

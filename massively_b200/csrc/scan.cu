@@ -6,18 +6,24 @@
 // about 16 bytes of traffic per u32) with one pass that reads the input once
 // and writes the output once (8 bytes per u32).
 //
-// Tile = 256 threads x 4 vectors of 16 bytes (4096 u32 / 2048 u64).  Each
-// warp owns a contiguous 512-item (256 for 64-bit) chunk and loads it with
-// coalesced 128-bit streaming loads: lane l holds vectors j*32 + l for
-// j = 0..3.  The scan runs serially over the vector, then as four warp
+// Tile = 256 threads x 4 vectors of 16 bytes (4096 u32 / 2048 u64, 16 KB).
+// Each warp owns a contiguous chunk; lane l holds vectors j*32 + l for
+// j = 0..3.  The scan runs serially over each vector, then as four warp
 // shuffle scans (one per vector row) and a fixed-order fold over the eight
-// warp totals.  Warp 0 then publishes the tile aggregate and runs the
-// look-back (lookback.cuh).  Operand order is preserved everywhere, so
+// warp totals.  Warp 0 publishes the tile aggregate and runs the look-back
+// (lookback.cuh).  Operand order is preserved everywhere, so
 // non-commutative operators (TAKE_LEFT) scan correctly.
+//
+// Plain aligned columns use the streaming kernel: persistent CTAs (a few per
+// SM) take tiles in order from an atomic ticket and keep the next tiles'
+// inputs in flight with cp.async.bulk copies into a 3-stage shared-memory
+// ring, so HBM keeps streaming while a tile waits in its look-back.  Lazy
+// views and device-length inputs use the one-tile-per-CTA kernel.
 //
 // Floating point: the association is a fixed tree inside the tile and the
 // deterministic fold across tiles, so results are identical run to run.
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "dispatch.cuh"
 #include "lookback.cuh"
@@ -28,6 +34,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kLoads = 4;
+constexpr int kStages = 3;
 
 template <class T>
 struct ScanCfg {
@@ -35,6 +42,7 @@ struct ScanCfg {
   static constexpr int ITEMS = VEC * kLoads;
   static constexpr int WARP_ITEMS = 32 * ITEMS;
   static constexpr int TILE = kThreads * ITEMS;
+  static constexpr int TILE_BYTES = TILE * (int)sizeof(T);
 };
 
 template <class T>
@@ -45,6 +53,12 @@ struct ScanParams {
   T init;
   uint32_t* counter;
   DevErr err;
+};
+
+template <class T>
+struct ScanShared {
+  T warp_total[kWarps];
+  T excl;
 };
 
 template <class T>
@@ -59,26 +73,117 @@ __device__ __forceinline__ void store_vec(T* p, uint64_t elem, const T (&src)[16
   __stcs(reinterpret_cast<uint4*>(p + elem), u);
 }
 
+// Scans one tile held in x (warp-striped vectors) into its final inclusive
+// (or exclusive) values.  Called by all threads of the CTA.
+template <class T, int OP, bool PACKED>
+__device__ __forceinline__ void scan_tile(T (&x)[kLoads][16 / sizeof(T)], uint64_t tile,
+                                          const ScanParams<T>& p,
+                                          const TileState<T, PACKED>& st, ScanShared<T>& sh) {
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr bool DET = std::is_floating_point<T>::value;
+  const Op<T, OP> op{p.op};
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+    for (int k = 1; k < VEC; ++k) x[j][k] = op(x[j][k - 1], x[j][k]);
+
+  T ge[kLoads];
+  T rowtot[kLoads];
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j) {
+    T g = x[j][VEC - 1];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      T o = shfl_up(g, d);
+      if (lane >= d) g = op(o, g);
+    }
+    rowtot[j] = shfl_idx(g, 31);
+    ge[j] = shfl_up(g, 1);
+  }
+  T rp[kLoads];
+  rp[0] = rowtot[0];
+#pragma unroll
+  for (int j = 1; j < kLoads; ++j) rp[j] = op(rp[j - 1], rowtot[j]);
+  if (lane == 0) sh.warp_total[warp] = rp[kLoads - 1];
+  __syncthreads();
+
+  if (warp == 0) {
+    T agg = sh.warp_total[0];
+#pragma unroll
+    for (int w = 1; w < kWarps; ++w) agg = op(agg, sh.warp_total[w]);
+    if (tile == 0) {
+      if (lane == 0) st.publish(0, kFlagIncl, agg);
+    } else {
+      if (lane == 0) st.publish(tile, kFlagAgg, agg);
+      T excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.err, agg);
+      if (lane == 0) {
+        st.publish(tile, kFlagIncl, op(excl, agg));
+        sh.excl = excl;
+      }
+    }
+  }
+  __syncthreads();
+
+  bool has_pre = tile > 0;
+  T pre = has_pre ? sh.excl : T(0);
+  for (int w = 0; w < warp; ++w) {
+    T t = sh.warp_total[w];
+    pre = has_pre ? op(pre, t) : t;
+    has_pre = true;
+  }
+
+  T y[kLoads][VEC];
+#pragma unroll
+  for (int j = 0; j < kLoads; ++j) {
+    bool h = has_pre;
+    T pj = pre;
+    if (j > 0) { pj = h ? op(pj, rp[j - 1]) : rp[j - 1]; h = true; }
+    if (lane > 0) { pj = h ? op(pj, ge[j]) : ge[j]; h = true; }
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) y[j][k] = h ? op(pj, x[j][k]) : x[j][k];
+  }
+
+  if (p.exclusive) {
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      T up = shfl_up(y[j][VEC - 1], 1);
+      T wrap = shfl_idx(j > 0 ? y[j - 1][VEC - 1] : y[0][VEC - 1], 31);
+      bool h0;
+      T prev0;
+      if (lane > 0) { prev0 = up; h0 = true; }
+      else if (j > 0) { prev0 = wrap; h0 = true; }
+      else { prev0 = pre; h0 = has_pre; }
+#pragma unroll
+      for (int k = VEC - 1; k >= 1; --k) x[j][k] = op(p.init, y[j][k - 1]);
+      x[j][0] = h0 ? op(p.init, prev0) : p.init;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) x[j][k] = y[j][k];
+  }
+}
+
+// One tile per CTA: lazy views, device-length inputs, unaligned columns.
 template <class T, int OP, bool PLAIN, bool PACKED>
 __global__ void __launch_bounds__(kThreads)
     scan_kernel(Src in, void* out, uint64_t cap, ScanParams<T> p, TileState<T, PACKED> st) {
   using C = ScanCfg<T>;
   constexpr int VEC = C::VEC;
-  constexpr bool DET = std::is_floating_point<T>::value;
   __shared__ uint32_t s_tile;
-  __shared__ T s_warp_total[kWarps];
-  __shared__ T s_excl;
+  __shared__ ScanShared<T> sh;
 
   if (threadIdx.x == 0) s_tile = atomicAdd(p.counter, 1u);
   __syncthreads();
   const uint64_t tile = s_tile;
-  uint64_t n = in.len_dev ? min((uint64_t)*in.len_dev, cap) : cap;
+  const uint64_t n = in.len_dev ? min((uint64_t)*in.len_dev, cap) : cap;
   const uint64_t tile_base = tile * (uint64_t)C::TILE;
   if (tile_base >= n) return;
-
-  const Op<T, OP> op{p.op};
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t warp_base = tile_base + (uint64_t)warp * C::WARP_ITEMS;
   const bool full = tile_base + C::TILE <= n;
 
@@ -101,96 +206,7 @@ __global__ void __launch_bounds__(kThreads)
         }
       }
   }
-
-  // Serial inclusive scan of each vector.
-#pragma unroll
-  for (int j = 0; j < kLoads; ++j)
-#pragma unroll
-    for (int k = 1; k < VEC; ++k) x[j][k] = op(x[j][k - 1], x[j][k]);
-
-  // Per row j: warp inclusive scan of the vector totals.
-  T ge[kLoads];     // lane-exclusive prefix within row j (valid for lane > 0)
-  T rowtot[kLoads];
-#pragma unroll
-  for (int j = 0; j < kLoads; ++j) {
-    T g = x[j][VEC - 1];
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      T o = shfl_up(g, d);
-      if (lane >= d) g = op(o, g);
-    }
-    rowtot[j] = shfl_idx(g, 31);
-    ge[j] = shfl_up(g, 1);
-  }
-  // Prefix of each row inside the warp chunk; the warp total.
-  T rp[kLoads];
-  rp[0] = rowtot[0];
-#pragma unroll
-  for (int j = 1; j < kLoads; ++j) rp[j] = op(rp[j - 1], rowtot[j]);
-  // rp[j] is now the inclusive total through row j; row j's prefix is rp[j-1].
-  if (lane == 0) s_warp_total[warp] = rp[kLoads - 1];
-  __syncthreads();
-
-  if (warp == 0) {
-    T agg = s_warp_total[0];
-#pragma unroll
-    for (int w = 1; w < kWarps; ++w) agg = op(agg, s_warp_total[w]);
-    if (tile == 0) {
-      if (lane == 0) st.publish(0, kFlagIncl, agg);
-    } else {
-      if (lane == 0) st.publish(tile, kFlagAgg, agg);
-      T excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.err, agg);
-      if (lane == 0) {
-        st.publish(tile, kFlagIncl, op(excl, agg));
-        s_excl = excl;
-      }
-    }
-  }
-  __syncthreads();
-
-  // Prefix of this warp's chunk: tile exclusive, then earlier warps in order.
-  bool has_pre = tile > 0;
-  T pre = has_pre ? s_excl : T(0);
-  for (int w = 0; w < warp; ++w) {
-    T t = s_warp_total[w];
-    pre = has_pre ? op(pre, t) : t;
-    has_pre = true;
-  }
-
-  // Final inclusive values.
-  T y[kLoads][VEC];
-#pragma unroll
-  for (int j = 0; j < kLoads; ++j) {
-    bool h = has_pre;
-    T pj = pre;
-    if (j > 0) { pj = h ? op(pj, rp[j - 1]) : rp[j - 1]; h = true; }
-    if (lane > 0) { pj = h ? op(pj, ge[j]) : ge[j]; h = true; }
-#pragma unroll
-    for (int k = 0; k < VEC; ++k) y[j][k] = h ? op(pj, x[j][k]) : x[j][k];
-  }
-
-  if (p.exclusive) {
-    const Op<T, OP> eop{p.op};
-#pragma unroll
-    for (int j = 0; j < kLoads; ++j) {
-      T up = shfl_up(y[j][VEC - 1], 1);
-      T wrap = shfl_idx(j > 0 ? y[j - 1][VEC - 1] : y[0][VEC - 1], 31);
-      bool h0;
-      T prev0;
-      if (lane > 0) { prev0 = up; h0 = true; }
-      else if (j > 0) { prev0 = wrap; h0 = true; }
-      else { prev0 = pre; h0 = has_pre; }
-#pragma unroll
-      for (int k = VEC - 1; k >= 1; --k) x[j][k] = eop(p.init, y[j][k - 1]);
-      x[j][0] = h0 ? eop(p.init, prev0) : p.init;
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < kLoads; ++j)
-#pragma unroll
-      for (int k = 0; k < VEC; ++k) x[j][k] = y[j][k];
-  }
-
+  scan_tile<T, OP, PACKED>(x, tile, p, st, sh);
   if (PLAIN && full) {
 #pragma unroll
     for (int j = 0; j < kLoads; ++j)
@@ -207,6 +223,93 @@ __global__ void __launch_bounds__(kThreads)
         }
       }
   }
+}
+
+// Persistent streaming kernel for plain 16-byte-aligned columns.
+template <class T, int OP, bool PACKED>
+__global__ void __launch_bounds__(kThreads)
+    scan_stream_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
+                       uint64_t ntiles, ScanParams<T> p, TileState<T, PACKED> st) {
+  using C = ScanCfg<T>;
+  constexpr int VEC = C::VEC;
+  extern __shared__ __align__(128) unsigned char scan_smem[];
+  T* ring = reinterpret_cast<T*>(scan_smem);  // kStages tiles
+  __shared__ __align__(8) uint64_t bar[kStages];
+  __shared__ uint32_t s_tile[kStages];
+  __shared__ ScanShared<T> sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // Acquires the next tile for ring slot s and starts its copy (thread 0).
+  auto issue = [&](int s) {
+    const uint32_t t = atomicAdd(p.counter, 1u);
+    s_tile[s] = t;
+    if (t < ntiles && (uint64_t)(t + 1) * C::TILE <= n) {
+      mbar_arrive_expect_tx(&bar[s], C::TILE_BYTES);
+      bulk_load(ring + (size_t)s * C::TILE, in + (uint64_t)t * C::TILE, C::TILE_BYTES, &bar[s]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bar[s], 1);
+    mbar_init_fence();
+    for (int s = 0; s < kStages; ++s) issue(s);
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  for (int it = 0;; ++it) {
+    const int s = it % kStages;
+    const uint64_t tile = s_tile[s];
+    if (tile >= ntiles) break;
+    const uint64_t tile_base = tile * (uint64_t)C::TILE;
+    const bool full = tile_base + C::TILE <= n;
+    const uint64_t warp_base = tile_base + (uint64_t)warp * C::WARP_ITEMS;
+    T x[kLoads][VEC];
+    if (full) {
+      if (!mbar_wait(&bar[s], (parity >> s) & 1u)) raise_device_error(p.err, MB_DEV_ERR_LOOKBACK);
+      parity ^= 1u << s;
+      const T* tb = ring + (size_t)s * C::TILE + warp * C::WARP_ITEMS;
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j) {
+        uint4 u = *reinterpret_cast<const uint4*>(tb + (j * 32 + lane) * VEC);
+        memcpy(x[j], &u, 16);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
+          x[j][k] = i < n ? in[i] : T(0);
+        }
+    }
+    scan_tile<T, OP, PACKED>(x, tile, p, st, sh);
+    if (full) {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+        store_vec<T>(out, warp_base + (uint64_t)(j * 32 + lane) * VEC, x[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
+          if (i < n) out[i] = x[j][k];
+        }
+    }
+    __syncthreads();  // ring slot s and `sh` are free again
+    if (threadIdx.x == 0) {
+      fence_proxy_async_smem();
+      issue(s);
+    }
+  }
+}
+
+int stream_grid(const void* kernel, size_t smem, uint64_t ntiles, int device) {
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+  if (per_sm < 1) per_sm = 1;
+  uint64_t g = (uint64_t)sms * per_sm;
+  return (int)(g < ntiles ? g : ntiles);
 }
 
 template <class T>
@@ -232,14 +335,22 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
   auto st = TileState<T, PACKED>::make(scratch.as<char>() + 256, tiles);
   const bool plain = src_plain(in, DTypeOf<T>::value) && out.dtype == DTypeOf<T>::value &&
                      ((uintptr_t)in.data % 16 == 0) && ((uintptr_t)out.data % 16 == 0);
+  const bool stream = plain && in.len_dev == nullptr;
   const Src s = to_src(in);
   dim3 grid(grid_for(tiles)), block(kThreads);
-#define MB_SCAN_LAUNCH(OPID)                                                               \
-  do {                                                                                     \
-    if (plain)                                                                             \
+  const size_t ring = (size_t)kStages * C::TILE_BYTES;
+#define MB_SCAN_LAUNCH(OPID)                                                                    \
+  do {                                                                                          \
+    if (stream) {                                                                               \
+      auto k = scan_stream_kernel<T, OPID, PACKED>;                                             \
+      MB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring)); \
+      const int g = stream_grid((const void*)k, ring, tiles, ex->device);                      \
+      k<<<g, kThreads, ring, ex->stream>>>((const T*)in.data, (T*)out.data, cap, tiles, p, st); \
+    } else if (plain) {                                                                         \
       scan_kernel<T, OPID, true, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
-    else                                                                                   \
+    } else {                                                                                    \
       scan_kernel<T, OPID, false, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
+    }                                                                                           \
   } while (0)
   switch (op) {
     case MB_OP_ADD: MB_SCAN_LAUNCH(MB_OP_ADD); break;

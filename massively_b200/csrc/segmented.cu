@@ -481,6 +481,43 @@ __global__ void segment_ids_kernel(const uint32_t* off, uint64_t nseg, uint32_t*
   }
 }
 
+__global__ void lengths_kernel(const uint32_t* off, uint64_t nseg, uint32_t* len) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
+       s += (uint64_t)gridDim.x * blockDim.x)
+    len[s] = off[s + 1] - off[s];
+}
+
+__global__ void local_indices_kernel(const uint32_t* off, uint64_t nseg, uint32_t* local,
+                                     uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    local[i] = (uint32_t)(i - off[upper_bound_u32(off, nseg + 1, i) - 1]);
+}
+
+// ids must be non-decreasing and < nseg; bad[0] is set otherwise.
+__global__ void validate_ids_kernel(Src ids, uint64_t n, uint64_t nseg, uint32_t* bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = src_load<uint32_t>(ids, i);
+    if (v >= nseg || (i > 0 && src_load<uint32_t>(ids, i - 1) > v)) atomicMax(bad, 1u);
+  }
+}
+
+// offsets[s] = first index i with ids[i] >= s (massively's lower_bound of
+// counting(0) against the ids).
+__global__ void offsets_from_ids_kernel(Src ids, uint64_t n, uint64_t nseg, uint32_t* off) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s <= nseg;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if ((uint64_t)src_load<uint32_t>(ids, mid) < s) lo = mid + 1;
+      else hi = mid;
+    }
+    off[s] = (uint32_t)lo;
+  }
+}
+
 unsigned grid_for_n(uint64_t n) {
   uint64_t g = (n + 255) / 256;
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 8));
@@ -565,6 +602,52 @@ int mb_segmentation_segment_ids(mb_executor* ex, const uint32_t* offsets, uint64
   if (value_count == 0) return MB_OK;
   segment_ids_kernel<<<grid_for_n(value_count), 256, 0, ex->stream>>>(offsets, segment_count, ids,
                                                                      value_count);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int mb_segmentation_lengths(mb_executor* ex, const uint32_t* offsets, uint64_t segment_count,
+                            uint32_t* lengths) {
+  MB_TRY(check_exec(ex));
+  if (segment_count == 0) return MB_OK;
+  lengths_kernel<<<grid_for_n(segment_count), 256, 0, ex->stream>>>(offsets, segment_count, lengths);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int mb_segmentation_local_indices(mb_executor* ex, const uint32_t* offsets,
+                                  uint64_t segment_count, uint32_t* local, uint64_t value_count) {
+  MB_TRY(check_exec(ex));
+  if (value_count == 0) return MB_OK;
+  local_indices_kernel<<<grid_for_n(value_count), 256, 0, ex->stream>>>(offsets, segment_count,
+                                                                       local, value_count);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int mb_segmentation_from_segment_ids(mb_executor* ex, const mb_src* ids, uint64_t segment_count,
+                                     uint32_t* offsets) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, ids, "segment ids"));
+  if (segment_count >= 0xFFFFFFFFull)
+    return set_error(MB_ERR_LENGTH_TOO_LARGE, "length does not fit in u32", segment_count + 1);
+  if (compute_type(ids->vtype) != MB_U32 || dtype_size(ids->vtype) != 4)
+    return set_error(MB_ERR_LAUNCH, "segment ids must be u32");
+  const uint64_t n = ids->len;
+  const Src s = to_src(*ids);
+  if (n > 0) {
+    Scratch bad;
+    MB_TRY(bad.alloc(ex, 16));
+    MB_CUDA(cudaMemsetAsync(bad.ptr, 0, 16, ex->stream));
+    validate_ids_kernel<<<grid_for_n(n), 256, 0, ex->stream>>>(s, n, segment_count,
+                                                             bad.as<uint32_t>());
+    MB_CUDA(cudaGetLastError());
+    uint32_t b = 0;
+    MB_TRY(read_u32(ex, bad.as<uint32_t>(), &b));
+    if (b) return set_error(MB_ERR_INVALID_SEGMENTATION, "segmentation is not a valid ordered partition");
+  }
+  offsets_from_ids_kernel<<<grid_for_n(segment_count + 1), 256, 0, ex->stream>>>(
+      s, n, segment_count, offsets);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }

@@ -50,17 +50,21 @@ unsigned grid_of(uint64_t n) {
 
 // out[i] = order-preserving unsigned encoding of view element i
 // (inverted for descending order).
-template <class K>
+// Keys are read as raw bits of their element type (narrow signed types
+// sign-extended to 32 bits) and encoded as integers.
+template <class U, int ENC>
 __global__ void __launch_bounds__(kThreads)
-    encode_keys_kernel(Src in, typename UnsignedOf<K>::type* out, uint64_t n, int ieee, int desc) {
-  using U = typename UnsignedOf<K>::type;
+    encode_keys_kernel(Src in, U* out, uint64_t n, int ieee, int desc) {
+  constexpr U sign = (U)1 << (sizeof(U) * 8 - 1);
   for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * kThreads) {
-    K k = src_load<K>(in, i);
-    if constexpr (std::is_floating_point<K>::value) {
-      if (ieee && k == K(0)) k = K(0);  // -0 == +0 under `<`
+    U raw = (U)src_load_bits(in, i);
+    if (in.vtype == MB_I8) raw = (U)(uint32_t)(int32_t)(int8_t)raw;
+    if (in.vtype == MB_I16) raw = (U)(uint32_t)(int32_t)(int16_t)raw;
+    if constexpr (ENC == kEncFloat) {
+      if (ieee && (raw & ~sign) == 0) raw = 0;  // -0 == +0 under `<`
     }
-    U u = radix_enc<K>(k);
+    const U u = enc_bits<U, ENC>(raw);
     out[i] = desc ? (U)~u : u;
   }
 }
@@ -80,10 +84,9 @@ bool wide_key_type(int dt) {
          dt == MB_F64;
 }
 
-template <class K>
+template <class U, int ENC>
 int encode_run(mb_executor* ex, const Src& s, void* out, uint64_t n, int ieee, int desc) {
-  encode_keys_kernel<K><<<grid_of(n), kThreads, 0, ex->stream>>>(
-      s, (typename UnsignedOf<K>::type*)out, n, ieee, desc);
+  encode_keys_kernel<U, ENC><<<grid_of(n), kThreads, 0, ex->stream>>>(s, (U*)out, n, ieee, desc);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -91,12 +94,12 @@ int encode_run(mb_executor* ex, const Src& s, void* out, uint64_t n, int ieee, i
 int encode_keys(mb_executor* ex, const Src& s, int vtype, void* out, uint64_t n, int ieee,
                 int desc) {
   switch (compute_type(vtype)) {
-    case MB_U32: return encode_run<uint32_t>(ex, s, out, n, ieee, desc);
-    case MB_I32: return encode_run<int32_t>(ex, s, out, n, ieee, desc);
-    case MB_F32: return encode_run<float>(ex, s, out, n, ieee, desc);
-    case MB_U64: return encode_run<uint64_t>(ex, s, out, n, ieee, desc);
-    case MB_I64: return encode_run<int64_t>(ex, s, out, n, ieee, desc);
-    case MB_F64: return encode_run<double>(ex, s, out, n, ieee, desc);
+    case MB_U32: return encode_run<uint32_t, kEncUnsigned>(ex, s, out, n, ieee, desc);
+    case MB_I32: return encode_run<uint32_t, kEncSigned>(ex, s, out, n, ieee, desc);
+    case MB_F32: return encode_run<uint32_t, kEncFloat>(ex, s, out, n, ieee, desc);
+    case MB_U64: return encode_run<uint64_t, kEncUnsigned>(ex, s, out, n, ieee, desc);
+    case MB_I64: return encode_run<uint64_t, kEncSigned>(ex, s, out, n, ieee, desc);
+    case MB_F64: return encode_run<uint64_t, kEncFloat>(ex, s, out, n, ieee, desc);
     default: return set_error(MB_ERR_LAUNCH, "unsupported key type");
   }
 }

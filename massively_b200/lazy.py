@@ -181,24 +181,21 @@ class Map(View):
 
 class AdjacentDifference(View):
     """lazy::adjacent_difference(input, op): out[0] = x[0], out[i] =
-    op(x[i-1], x[i]); lowered by materialising (one fused copy kernel)."""
+    op(x[i-1], x[i]), evaluated inside the consuming kernel's load
+    (MB_SRC_ADJACENT)."""
 
     def __init__(self, values, reduction):
         self.values, self.op = values, O.reduction(reduction)
         self.dtype, self.len = values.dtype, len(values)
 
     def lower(self, exec, keep):
-        x = _as_column(exec, self.values, keep)
-        t = x.tensor
-        out = exec.alloc(self.dtype, len(x))
-        if len(x):
-            out.tensor[:1] = t[:1]
-            if len(x) > 1:
-                from .vector import _binary_elementwise
-                _binary_elementwise(exec, x.slice(0, len(x) - 1), x.slice(1), self.op,
-                                    out.slice(1))
-        keep.append(out)
-        return out.to_src()
+        col = _as_column(exec, self.values, keep)
+        s = col.to_src()
+        s.kind = N.SRC_ADJACENT
+        s.b = self.op.id
+        s.len = self.len
+        s.len_dev = None
+        return s
 
 
 def constant(value, dtype=None) -> Constant:

@@ -61,21 +61,12 @@ class Segmentation:
         non-decreasing and < segment_count."""
         if segment_count >= MINDEX_MAX:
             raise LengthTooLarge(segment_count + 1)
-        idv = _u32_column(exec, ids)
-        t = idv.tensor
-        if len(idv):
-            bad = (t[-1:].to(__import__("torch").int64) >= segment_count).any()
-            if len(idv) > 1:
-                bad = bad | (t[1:].to(__import__("torch").int64) <
-                             t[:-1].to(__import__("torch").int64)).any()
-            if bool(bad):
-                raise InvalidSegmentation()
-        import torch
-        counts = torch.bincount(t.to(torch.int64), minlength=segment_count) if len(idv) else \
-            torch.zeros(segment_count, dtype=torch.int64, device=t.device)
-        off = torch.zeros(segment_count + 1, dtype=torch.int64, device=t.device)
-        off[1:] = torch.cumsum(counts, 0)
-        return cls(exec.from_tensor(off.to(torch.uint32)), len(idv))
+        keep = []
+        s = lower(exec, ids, keep)
+        off = exec.alloc(U32, segment_count + 1)
+        check(_L().mb_segmentation_from_segment_ids(exec.handle, C.byref(s), segment_count,
+                                                    C.c_void_p(off.data_ptr())))
+        return cls(off, len(ids))
 
     def offsets(self) -> DeviceVec:
         return self._offsets
@@ -87,10 +78,12 @@ class Segmentation:
         return self._value_count
 
     def lengths(self, exec: Executor) -> DeviceVec:
-        t = self._offsets.tensor
-        import torch
-        d = (t[1:].to(torch.int64) - t[:-1].to(torch.int64)).to(torch.uint32)
-        return exec.from_tensor(d.contiguous())
+        """Segmentation::lengths: one length per segment."""
+        out = exec.alloc(U32, self.segment_count())
+        if self.segment_count():
+            check(_L().mb_segmentation_lengths(exec.handle, C.c_void_p(self._offsets.data_ptr()),
+                                               self.segment_count(), C.c_void_p(out.data_ptr())))
+        return out
 
     def segment_ids(self, exec: Executor) -> DeviceVec:
         """Segmentation::segment_ids: flat value -> segment index."""
@@ -102,11 +95,13 @@ class Segmentation:
         return out
 
     def local_indices(self, exec: Executor) -> DeviceVec:
-        ids = self.segment_ids(exec)
-        import torch
-        pos = torch.arange(self._value_count, device=ids.tensor.device, dtype=torch.int64)
-        starts = self._offsets.tensor.to(torch.int64)[ids.tensor.to(torch.int64)]
-        return exec.from_tensor((pos - starts).to(torch.uint32))
+        """Segmentation::local_indices: position of each value in its segment."""
+        out = exec.alloc(U32, self._value_count)
+        if self._value_count:
+            check(_L().mb_segmentation_local_indices(
+                exec.handle, C.c_void_p(self._offsets.data_ptr()), self.segment_count(),
+                C.c_void_p(out.data_ptr()), self._value_count))
+        return out
 
     def segments(self, values) -> "SegmentIterator":
         if len(values) != self._value_count:

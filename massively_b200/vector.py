@@ -113,27 +113,6 @@ def fill(exec: Executor, value, output: DeviceVec) -> None:
     check(_L().mb_fill(exec.handle, buf, output.to_col()))
 
 
-def _binary_elementwise(exec, left, right, op, out):
-    """out[i] = op(left[i], right[i]) -- used to lower adjacent_difference."""
-    o = O.reduction(op)
-    a, b = left.tensor, right.tensor
-    if o.name == "add":
-        r = a + b
-    elif o.name == "mul":
-        r = a * b
-    elif o.name == "min":
-        r = torch.where(b < a, b, a)
-    elif o.name == "max":
-        r = torch.where(a < b, b, a)
-    elif o.name == "take_left":
-        r = a
-    elif o.name == "take_right":
-        r = b
-    else:
-        r = {"and": torch.bitwise_and, "or": torch.bitwise_or, "xor": torch.bitwise_xor}[o.name](a, b)
-    out.tensor.copy_(r)
-
-
 # ----------------------------------------------------------------- scan --
 
 def inclusive_scan(exec: Executor, input, op) -> DeviceVec:
