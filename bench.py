@@ -462,6 +462,8 @@ def run_ours(args):
                              device_id=torch.device(f"cuda:{local}"))
     import massively_b200 as mb
     ex = mb.Executor(local)
+    from massively_b200 import tune
+    tune.apply(ex)  # persisted autotuner choices (or MB_TUNE_<FAMILY> overrides)
     wl = WORKLOADS[args.workload]()
     wl.setup(ex)
     torch.cuda.synchronize()

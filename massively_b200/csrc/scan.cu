@@ -6,22 +6,25 @@
 // about 16 bytes of traffic per u32) with one pass that reads the input once
 // and writes the output once (8 bytes per u32).
 //
-// Tile = 256 threads x 4 vectors of 16 bytes (4096 u32 / 2048 u64, 16 KB).
-// Each warp owns a contiguous chunk; lane l holds vectors j*32 + l for
-// j = 0..3.  The scan runs serially over each vector, then as four warp
-// shuffle scans (one per vector row) and a fixed-order fold over the eight
-// warp totals.  Warp 0 publishes the tile aggregate and runs the look-back
-// (lookback.cuh).  Operand order is preserved everywhere, so
-// non-commutative operators (TAKE_LEFT) scan correctly.
-//
-// Plain aligned columns use the streaming kernel: persistent CTAs (a few per
-// SM) take tiles in order from an atomic ticket and keep the next tiles'
-// inputs in flight with cp.async.bulk copies into a 3-stage shared-memory
-// ring, so HBM keeps streaming while a tile waits in its look-back.  Lazy
-// views and device-length inputs use the one-tile-per-CTA kernel.
-//
-// Floating point: the association is a fixed tree inside the tile and the
-// deterministic fold across tiles, so results are identical run to run.
+// Plain 16-byte-aligned columns (the streaming path): one CTA per 32 KB tile.
+// Thread 0 fetches the whole tile into shared memory with one cp.async.bulk
+// copy (TMA, completion on an mbarrier), so the bytes in flight do not cost
+// registers and many tiles per SM can be loading while others wait in their
+// look-back.  The tile is scanned in place in three phases:
+//   1. per warp, row by row (a row = 32 lanes x one 16-byte vector): serial
+//      scan of the vector, warp shuffle scan of the vector totals, carry from
+//      the previous row; the warp-local inclusive values go back to shared
+//      memory;
+//   2. warp 0 folds the eight warp totals in order, publishes the tile
+//      aggregate and runs the look-back (lookback.cuh), giving every warp its
+//      prefix;
+//   3. every value is combined with its warp prefix on the way out to global
+//      memory (16-byte streaming stores).
+// Lazy views and device-length inputs use a register-tiled kernel with the
+// same arithmetic structure.  Operand order is preserved everywhere, so
+// non-commutative operators (TAKE_LEFT) scan correctly; floating-point
+// association is a fixed tree inside the tile plus the deterministic fold
+// across tiles, so results are identical run to run.
 
 #include "bulk.cuh"
 #include "common.cuh"
@@ -33,8 +36,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kLoads = 4;
-constexpr int kStages = 3;
+constexpr int kLoads = 4;  // register-tiled kernel: vectors per thread
+constexpr int kRows = 8;   // smem kernel: vector rows per warp
 
 template <class T>
 struct ScanCfg {
@@ -42,6 +45,13 @@ struct ScanCfg {
   static constexpr int ITEMS = VEC * kLoads;
   static constexpr int WARP_ITEMS = 32 * ITEMS;
   static constexpr int TILE = kThreads * ITEMS;
+};
+
+template <class T>
+struct SmemCfg {
+  static constexpr int VEC = 16 / sizeof(T);
+  static constexpr int WARP_ITEMS = 32 * kRows * VEC;
+  static constexpr int TILE = kWarps * WARP_ITEMS;  // 32 KB
   static constexpr int TILE_BYTES = TILE * (int)sizeof(T);
 };
 
@@ -73,8 +83,151 @@ __device__ __forceinline__ void store_vec(T* p, uint64_t elem, const T (&src)[16
   __stcs(reinterpret_cast<uint4*>(p + elem), u);
 }
 
-// Scans one tile held in x (warp-striped vectors) into its final inclusive
-// (or exclusive) values.  Called by all threads of the CTA.
+// Warp 0: folds the warp totals, publishes the tile, runs the look-back and
+// writes each warp's prefix (pre[w], has[w]).
+template <class T, int OP, bool PACKED>
+__device__ __forceinline__ void tile_prefixes(uint64_t tile, const ScanParams<T>& p,
+                                              const TileState<T, PACKED>& st, const T* wtot,
+                                              T* pre, bool* has) {
+  constexpr bool DET = std::is_floating_point<T>::value;
+  const Op<T, OP> op{p.op};
+  const int lane = threadIdx.x & 31;
+  T agg = wtot[0];
+#pragma unroll
+  for (int w = 1; w < kWarps; ++w) agg = op(agg, wtot[w]);
+  T excl = agg;
+  if (tile == 0) {
+    if (lane == 0) st.publish(0, kFlagIncl, agg);
+  } else {
+    if (lane == 0) st.publish(tile, kFlagAgg, agg);
+    excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.err, agg);
+    if (lane == 0) st.publish(tile, kFlagIncl, op(excl, agg));
+  }
+  if (lane == 0) {
+    bool h = tile > 0;
+    T acc = excl;
+    for (int w = 0; w < kWarps; ++w) {
+      pre[w] = acc;
+      has[w] = h;
+      acc = h ? op(acc, wtot[w]) : wtot[w];
+      h = true;
+    }
+  }
+}
+
+template <class T, int OP, bool PACKED>
+__global__ void __launch_bounds__(kThreads)
+    scan_smem_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
+                     ScanParams<T> p, TileState<T, PACKED> st) {
+  using C = SmemCfg<T>;
+  constexpr int VEC = C::VEC;
+  extern __shared__ __align__(128) unsigned char scan_smem[];
+  T* buf = reinterpret_cast<T*>(scan_smem);
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t s_tile;
+  __shared__ T s_wtot[kWarps];
+  __shared__ T s_pre[kWarps];
+  __shared__ bool s_has[kWarps];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(p.counter, 1u);
+    s_tile = t;
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+    if ((uint64_t)(t + 1) * C::TILE <= n) {
+      mbar_arrive_expect_tx(&bar, C::TILE_BYTES);
+      bulk_load(buf, in + (uint64_t)t * C::TILE, C::TILE_BYTES, &bar);
+    }
+  }
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t tile_base = tile * (uint64_t)C::TILE;
+  if (tile_base >= n) return;
+  const bool full = tile_base + C::TILE <= n;
+  if (full) {
+    if (!mbar_wait(&bar, 0)) raise_device_error(p.err, MB_DEV_ERR_LOOKBACK);
+  } else {
+    for (int i = threadIdx.x; i < C::TILE; i += kThreads)
+      buf[i] = tile_base + i < n ? in[tile_base + i] : T(0);
+    __syncthreads();
+  }
+
+  // Phase 1: warp-local inclusive scan, row by row, in place.
+  const Op<T, OP> op{p.op};
+  T* wb = buf + warp * C::WARP_ITEMS;
+  T carry = T(0);
+#pragma unroll 2
+  for (int j = 0; j < kRows; ++j) {
+    T v[VEC];
+    uint4 u = *reinterpret_cast<const uint4*>(wb + (j * 32 + lane) * VEC);
+    memcpy(v, &u, 16);
+#pragma unroll
+    for (int k = 1; k < VEC; ++k) v[k] = op(v[k - 1], v[k]);
+    T g = v[VEC - 1];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      T o = shfl_up(g, d);
+      if (lane >= d) g = op(o, g);
+    }
+    const T rowtot = shfl_idx(g, 31);
+    const T ge = shfl_up(g, 1);
+    bool h = j > 0;
+    T pj = carry;
+    if (lane > 0) { pj = h ? op(pj, ge) : ge; h = true; }
+    if (h) {
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) v[k] = op(pj, v[k]);
+    }
+    memcpy(&u, v, 16);
+    *reinterpret_cast<uint4*>(wb + (j * 32 + lane) * VEC) = u;
+    carry = j > 0 ? op(carry, rowtot) : rowtot;
+  }
+  if (lane == 0) s_wtot[warp] = carry;
+  __syncthreads();
+
+  // Phase 2: tile aggregate, look-back, warp prefixes.
+  if (warp == 0) tile_prefixes<T, OP, PACKED>(tile, p, st, s_wtot, s_pre, s_has);
+  __syncthreads();
+
+  // Phase 3: apply the warp prefix on the way out.
+  const T pre = s_pre[warp];
+  const bool has = s_has[warp];
+  const uint64_t wg = tile_base + (uint64_t)warp * C::WARP_ITEMS;
+#pragma unroll 2
+  for (int j = 0; j < kRows; ++j) {
+    const int li = (j * 32 + lane) * VEC;  // warp-local index of item 0
+    T v[VEC];
+    uint4 u = *reinterpret_cast<const uint4*>(wb + li);
+    memcpy(v, &u, 16);
+    T o[VEC];
+    if (p.exclusive) {
+      // Inclusive value of the item before each item, then init op it.
+      bool h0 = has;
+      T prev0 = pre;
+      if (li > 0) {
+        prev0 = has ? op(pre, wb[li - 1]) : wb[li - 1];
+        h0 = true;
+      }
+      o[0] = h0 ? op(p.init, prev0) : p.init;
+#pragma unroll
+      for (int k = 1; k < VEC; ++k) o[k] = op(p.init, has ? op(pre, v[k - 1]) : v[k - 1]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) o[k] = has ? op(pre, v[k]) : v[k];
+    }
+    if (full) {
+      store_vec<T>(out, wg + li, o);
+    } else {
+#pragma unroll
+      for (int k = 0; k < VEC; ++k)
+        if (wg + li + k < n) out[wg + li + k] = o[k];
+    }
+  }
+}
+
+// Register-tiled scan of one tile held in x (warp-striped vectors) into its
+// final inclusive (or exclusive) values.  Called by all threads of the CTA.
 template <class T, int OP, bool PACKED>
 __device__ __forceinline__ void scan_tile(T (&x)[kLoads][16 / sizeof(T)], uint64_t tile,
                                           const ScanParams<T>& p,
@@ -168,7 +321,8 @@ __device__ __forceinline__ void scan_tile(T (&x)[kLoads][16 / sizeof(T)], uint64
   }
 }
 
-// One tile per CTA: lazy views, device-length inputs, unaligned columns.
+// One tile per CTA in registers: lazy views, device-length inputs, unaligned
+// columns.
 template <class T, int OP, bool PLAIN, bool PACKED>
 __global__ void __launch_bounds__(kThreads)
     scan_kernel(Src in, void* out, uint64_t cap, ScanParams<T> p, TileState<T, PACKED> st) {
@@ -225,101 +379,17 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Persistent streaming kernel for plain 16-byte-aligned columns.
-template <class T, int OP, bool PACKED>
-__global__ void __launch_bounds__(kThreads)
-    scan_stream_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
-                       uint64_t ntiles, ScanParams<T> p, TileState<T, PACKED> st) {
-  using C = ScanCfg<T>;
-  constexpr int VEC = C::VEC;
-  extern __shared__ __align__(128) unsigned char scan_smem[];
-  T* ring = reinterpret_cast<T*>(scan_smem);  // kStages tiles
-  __shared__ __align__(8) uint64_t bar[kStages];
-  __shared__ uint32_t s_tile[kStages];
-  __shared__ ScanShared<T> sh;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // Acquires the next tile for ring slot s and starts its copy (thread 0).
-  auto issue = [&](int s) {
-    const uint32_t t = atomicAdd(p.counter, 1u);
-    s_tile[s] = t;
-    if (t < ntiles && (uint64_t)(t + 1) * C::TILE <= n) {
-      mbar_arrive_expect_tx(&bar[s], C::TILE_BYTES);
-      bulk_load(ring + (size_t)s * C::TILE, in + (uint64_t)t * C::TILE, C::TILE_BYTES, &bar[s]);
-    }
-  };
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bar[s], 1);
-    mbar_init_fence();
-    for (int s = 0; s < kStages; ++s) issue(s);
-  }
-  __syncthreads();
-  uint32_t parity = 0;
-  for (int it = 0;; ++it) {
-    const int s = it % kStages;
-    const uint64_t tile = s_tile[s];
-    if (tile >= ntiles) break;
-    const uint64_t tile_base = tile * (uint64_t)C::TILE;
-    const bool full = tile_base + C::TILE <= n;
-    const uint64_t warp_base = tile_base + (uint64_t)warp * C::WARP_ITEMS;
-    T x[kLoads][VEC];
-    if (full) {
-      if (!mbar_wait(&bar[s], (parity >> s) & 1u)) raise_device_error(p.err, MB_DEV_ERR_LOOKBACK);
-      parity ^= 1u << s;
-      const T* tb = ring + (size_t)s * C::TILE + warp * C::WARP_ITEMS;
-#pragma unroll
-      for (int j = 0; j < kLoads; ++j) {
-        uint4 u = *reinterpret_cast<const uint4*>(tb + (j * 32 + lane) * VEC);
-        memcpy(x[j], &u, 16);
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < kLoads; ++j)
-#pragma unroll
-        for (int k = 0; k < VEC; ++k) {
-          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
-          x[j][k] = i < n ? in[i] : T(0);
-        }
-    }
-    scan_tile<T, OP, PACKED>(x, tile, p, st, sh);
-    if (full) {
-#pragma unroll
-      for (int j = 0; j < kLoads; ++j)
-        store_vec<T>(out, warp_base + (uint64_t)(j * 32 + lane) * VEC, x[j]);
-    } else {
-#pragma unroll
-      for (int j = 0; j < kLoads; ++j)
-#pragma unroll
-        for (int k = 0; k < VEC; ++k) {
-          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
-          if (i < n) out[i] = x[j][k];
-        }
-    }
-    __syncthreads();  // ring slot s and `sh` are free again
-    if (threadIdx.x == 0) {
-      fence_proxy_async_smem();
-      issue(s);
-    }
-  }
-}
-
-int stream_grid(const void* kernel, size_t smem, uint64_t ntiles, int device) {
-  int sms = 148, per_sm = 1;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
-  if (per_sm < 1) per_sm = 1;
-  uint64_t g = (uint64_t)sms * per_sm;
-  return (int)(g < ntiles ? g : ntiles);
-}
-
 template <class T>
 int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const void* init,
              const mb_col& out) {
-  using C = ScanCfg<T>;
   constexpr bool PACKED = sizeof(T) == 4;
   const uint64_t cap = in.len;
   if (cap == 0) return MB_OK;
-  const uint64_t tiles = (cap + C::TILE - 1) / C::TILE;
+  const bool plain = src_plain(in, DTypeOf<T>::value) && out.dtype == DTypeOf<T>::value &&
+                     ((uintptr_t)in.data % 16 == 0) && ((uintptr_t)out.data % 16 == 0);
+  const bool smem_path = plain && in.len_dev == nullptr;
+  const uint64_t tile_items = smem_path ? SmemCfg<T>::TILE : ScanCfg<T>::TILE;
+  const uint64_t tiles = (cap + tile_items - 1) / tile_items;
   Scratch scratch;
   const size_t state_bytes = TileState<T, PACKED>::bytes(tiles);
   MB_TRY(scratch.alloc(ex, 256 + state_bytes));
@@ -333,19 +403,14 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
   p.counter = scratch.as<uint32_t>();
   p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
   auto st = TileState<T, PACKED>::make(scratch.as<char>() + 256, tiles);
-  const bool plain = src_plain(in, DTypeOf<T>::value) && out.dtype == DTypeOf<T>::value &&
-                     ((uintptr_t)in.data % 16 == 0) && ((uintptr_t)out.data % 16 == 0);
-  const bool stream = plain && in.len_dev == nullptr;
   const Src s = to_src(in);
   dim3 grid(grid_for(tiles)), block(kThreads);
-  const size_t ring = (size_t)kStages * C::TILE_BYTES;
+  const size_t smem = SmemCfg<T>::TILE_BYTES;
 #define MB_SCAN_LAUNCH(OPID)                                                                    \
   do {                                                                                          \
-    if (stream) {                                                                               \
-      auto k = scan_stream_kernel<T, OPID, PACKED>;                                             \
-      MB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring)); \
-      const int g = stream_grid((const void*)k, ring, tiles, ex->device);                      \
-      k<<<g, kThreads, ring, ex->stream>>>((const T*)in.data, (T*)out.data, cap, tiles, p, st); \
+    if (smem_path) {                                                                            \
+      scan_smem_kernel<T, OPID, PACKED><<<grid, block, smem, ex->stream>>>(                     \
+          (const T*)in.data, (T*)out.data, cap, p, st);                                         \
     } else if (plain) {                                                                         \
       scan_kernel<T, OPID, true, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
     } else {                                                                                    \

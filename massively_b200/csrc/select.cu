@@ -152,116 +152,101 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
   }
 }
 
-// Persistent streaming variant of the fast path: one plain 4-byte column,
-// flags fused on it (FUSED) or read from a plain u32 stencil; the next tiles
-// of the inputs stream into a shared-memory ring with cp.async.bulk while a
-// tile waits in its look-back.
-constexpr int kStages = 3;
+// Fast path for plain 16-byte-aligned columns: one CTA per 32 KB tile of
+// one 4-byte column (plus its u32 stencil unless the predicate is fused on
+// the column).  Thread 0 fetches the tile(s) into shared memory with
+// cp.async.bulk, so bytes in flight cost no registers; the CTA counts its
+// kept rows from shared memory, runs the look-back, then re-evaluates the
+// flags from shared memory and writes the kept rows.
+constexpr int kSmemTile = 8192;  // 4-byte items per tile (32 KB)
+constexpr int kSmemItems = kSmemTile / kThreads;  // 32 per thread, warp-striped
 
 template <bool FUSED>
 __global__ void __launch_bounds__(kThreads)
-    select_stream_kernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ stencil,
-                         uint32_t* __restrict__ out, uint64_t n, uint64_t ntiles, int fused_map,
-                         int in_dtype, uint32_t invert, uint32_t* count_dev, uint32_t* counter,
-                         DevErr err, TileState<uint32_t, true> st) {
+    select_smem_kernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ stencil,
+                       uint32_t* __restrict__ out, uint64_t n, int fused_map, int in_dtype,
+                       uint32_t invert, uint32_t* count_dev, uint32_t* counter, DevErr err,
+                       TileState<uint32_t, true> st) {
   constexpr int kCols = FUSED ? 1 : 2;
-  constexpr int kTileBytes = kTile * 4;
+  constexpr int kTileBytes = kSmemTile * 4;
   extern __shared__ __align__(128) unsigned char sel_smem[];
-  uint32_t* ring = reinterpret_cast<uint32_t*>(sel_smem);  // [stage][col][kTile]
-  __shared__ __align__(8) uint64_t bar[kStages];
-  __shared__ uint32_t s_tile[kStages];
+  uint32_t* buf = reinterpret_cast<uint32_t*>(sel_smem);  // [col][kSmemTile]
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t s_tile;
   __shared__ uint32_t s_wcount[kWarps];
   __shared__ uint32_t s_excl;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  auto issue = [&](int s) {
-    const uint32_t t = atomicAdd(counter, 1u);
-    s_tile[s] = t;
-    if (t < ntiles && (uint64_t)(t + 1) * kTile <= n) {
-      mbar_arrive_expect_tx(&bar[s], kCols * kTileBytes);
-      uint32_t* dst = ring + (size_t)s * kCols * kTile;
-      bulk_load(dst, in + (uint64_t)t * kTile, kTileBytes, &bar[s]);
-      if constexpr (!FUSED) bulk_load(dst + kTile, stencil + (uint64_t)t * kTile, kTileBytes, &bar[s]);
-    }
-  };
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bar[s], 1);
+    const uint32_t t = atomicAdd(counter, 1u);
+    s_tile = t;
+    mbar_init(&bar, 1);
     mbar_init_fence();
-    for (int s = 0; s < kStages; ++s) issue(s);
+    if ((uint64_t)(t + 1) * kSmemTile <= n) {
+      mbar_arrive_expect_tx(&bar, kCols * kTileBytes);
+      bulk_load(buf, in + (uint64_t)t * kSmemTile, kTileBytes, &bar);
+      if constexpr (!FUSED)
+        bulk_load(buf + kSmemTile, stencil + (uint64_t)t * kSmemTile, kTileBytes, &bar);
+    }
   }
   __syncthreads();
-  uint32_t parity = 0;
-  for (int it = 0;; ++it) {
-    const int s = it % kStages;
-    const uint64_t tile = s_tile[s];
-    if (tile >= ntiles) break;
-    const uint64_t tile_base = tile * (uint64_t)kTile;
-    const bool full = tile_base + kTile <= n;
-    const uint64_t warp_base = tile_base + (uint64_t)warp * 32 * kItems;
-    const uint32_t* tv = ring + (size_t)s * kCols * kTile + warp * 32 * kItems;
-    if (full) {
-      if (!mbar_wait(&bar[s], (parity >> s) & 1u)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-      parity ^= 1u << s;
-    }
-    uint32_t v0[kItems];
-    unsigned ballot[kItems];
-    uint32_t wcount = 0;
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-      const uint64_t i = warp_base + (uint64_t)k * 32 + lane;
-      const bool valid = i < n;
-      uint32_t f = 0;
-      if (valid) {
-        uint32_t sv;
-        if (full) {
-          v0[k] = tv[k * 32 + lane];
-          sv = FUSED ? 0u : tv[kTile + k * 32 + lane];
-        } else {
-          v0[k] = in[i];
-          sv = FUSED ? 0u : stencil[i];
-        }
-        if constexpr (FUSED) f = map_to<uint32_t>(fused_map, in_dtype, v0[k]) != 0;
-        else f = sv != 0;
-        f ^= invert;
-      }
-      ballot[k] = __ballot_sync(kFull, valid && f);
-      wcount += __popc(ballot[k]);
-    }
-    if (lane == 0) s_wcount[warp] = wcount;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t c = lane < kWarps ? s_wcount[lane] : 0u;
-      uint32_t agg = __reduce_add_sync(kFull, c);
-      const Op<uint32_t, MB_OP_ADD> add{MB_OP_ADD};
-      uint32_t excl = 0;
-      if (tile == 0) {
-        if (lane == 0) st.publish(0, kFlagIncl, agg);
-      } else {
-        if (lane == 0) st.publish(tile, kFlagAgg, agg);
-        excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add, err, 0u);
-        if (lane == 0) st.publish(tile, kFlagIncl, excl + agg);
-      }
-      if (lane == 0) {
-        s_excl = excl;
-        if (tile_base + kTile >= n && count_dev) *count_dev = excl + agg;
-      }
+  const uint64_t tile = s_tile;
+  const uint64_t tile_base = tile * (uint64_t)kSmemTile;
+  if (tile_base >= n) return;
+  const bool full = tile_base + kSmemTile <= n;
+  if (full) {
+    if (!mbar_wait(&bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+  } else {
+    for (int i = threadIdx.x; i < kSmemTile; i += kThreads) {
+      const bool ok = tile_base + i < n;
+      buf[i] = ok ? in[tile_base + i] : 0u;
+      if constexpr (!FUSED) buf[kSmemTile + i] = ok ? stencil[tile_base + i] : 0u;
     }
     __syncthreads();
-    uint32_t run = s_excl;
-    for (int w = 0; w < warp; ++w) run += s_wcount[w];
-    const unsigned lt = (1u << lane) - 1u;
-#pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-      if ((ballot[k] >> lane) & 1u) out[run + __popc(ballot[k] & lt)] = v0[k];
-      run += __popc(ballot[k]);
+  }
+  const uint32_t* wv = buf + warp * 32 * kSmemItems;
+  const uint32_t* ws = wv + kSmemTile;
+  auto flag = [&](int k) -> bool {
+    const uint64_t i = tile_base + (uint64_t)warp * 32 * kSmemItems + k * 32 + lane;
+    if (i >= n) return false;
+    uint32_t f;
+    if constexpr (FUSED) f = map_to<uint32_t>(fused_map, in_dtype, wv[k * 32 + lane]) != 0;
+    else f = ws[k * 32 + lane] != 0;
+    return (f ^ invert) != 0;
+  };
+  uint32_t wcount = 0;
+#pragma unroll 8
+  for (int k = 0; k < kSmemItems; ++k) wcount += __popc(__ballot_sync(kFull, flag(k)));
+  if (lane == 0) s_wcount[warp] = wcount;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t c = lane < kWarps ? s_wcount[lane] : 0u;
+    uint32_t agg = __reduce_add_sync(kFull, c);
+    const Op<uint32_t, MB_OP_ADD> add{MB_OP_ADD};
+    uint32_t excl = 0;
+    if (tile == 0) {
+      if (lane == 0) st.publish(0, kFlagIncl, agg);
+    } else {
+      if (lane == 0) st.publish(tile, kFlagAgg, agg);
+      excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add, err, 0u);
+      if (lane == 0) st.publish(tile, kFlagIncl, excl + agg);
     }
-    __syncthreads();  // ring slot s, s_wcount and s_excl are free again
-    if (threadIdx.x == 0) {
-      fence_proxy_async_smem();
-      issue(s);
+    if (lane == 0) {
+      s_excl = excl;
+      if (tile_base + kSmemTile >= n && count_dev) *count_dev = excl + agg;
     }
   }
+  __syncthreads();
+  uint32_t run = s_excl;
+  for (int w = 0; w < warp; ++w) run += s_wcount[w];
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll 8
+  for (int k = 0; k < kSmemItems; ++k) {
+    const bool f = flag(k);
+    const unsigned b = __ballot_sync(kFull, f);
+    if (f) out[run + __popc(b & lt)] = wv[k * 32 + lane];
+    run += __popc(b);
+  }
 }
-
 int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* stencil,
                  const mb_col* out, uint32_t* count_dev, uint32_t* count_host, int mode,
                  uint32_t* boundary_dev) {
@@ -322,22 +307,18 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
                          (p.fused || (uintptr_t)stencil->data % 16 == 0);
     if (fast && aligned && mode != kPartition) {
       const int cols = p.fused ? 1 : 2;
-      const size_t ring = (size_t)kStages * cols * kTile * 4;
+      const size_t smem = (size_t)cols * kSmemTile * 4;
+      const uint64_t stiles = (n + kSmemTile - 1) / kSmemTile;
       auto launch = [&](auto kern) -> int {
-        MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring));
-        int sms = 148, per_sm = 1;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ex->device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, ring);
-        const uint64_t g = std::min<uint64_t>((uint64_t)sms * std::max(1, per_sm), tiles);
-        kern<<<(unsigned)g, kThreads, ring, ex->stream>>>(
+        MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<(unsigned)stiles, kThreads, smem, ex->stream>>>(
             (const uint32_t*)in[0].data, (const uint32_t*)stencil->data, (uint32_t*)out[0].data, n,
-            tiles, stencil->map, in[0].dtype, mode == kRemove ? 1u : 0u, count_dev, p.counter,
-            p.err, st);
+            stencil->map, in[0].dtype, mode == kRemove ? 1u : 0u, count_dev, p.counter, p.err, st);
         MB_CUDA(cudaGetLastError());
         return MB_OK;
       };
-      if (p.fused) MB_TRY(launch(select_stream_kernel<true>));
-      else MB_TRY(launch(select_stream_kernel<false>));
+      if (p.fused) MB_TRY(launch(select_smem_kernel<true>));
+      else MB_TRY(launch(select_smem_kernel<false>));
     } else if (fast)
       select_kernel<true><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
     else
