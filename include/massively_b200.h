@@ -217,6 +217,20 @@ int mb_fill(mb_executor* exec, const void* value, mb_col out);
 /* vector::inclusive_scan (massively/src/api/algorithm/scan.rs:96; core
  * massively/src/core/scan.rs:1125): out[i] = x0 op x1 op ... op xi. */
 int mb_inclusive_scan(mb_executor* exec, const mb_src* in, int op, mb_col out);
+/* Inclusive scan that allocates nothing.  No counterpart in massively: it
+ * exists for callers that must not allocate device memory during a call --
+ * for instance code that runs while another allocator owns all free device
+ * memory, or that has to be free of allocation failures and allocator
+ * synchronisation in the middle of its work.  Same result as
+ * mb_inclusive_scan; the look-back scratch lives in a fixed 1 MiB array in
+ * the library's device memory (every device that loads the library holds it
+ * until exit) instead of the pool.  Limit: at most 2^27 elements of a 4-byte
+ * type or 2^26 of an 8-byte type (MB_ERR_LENGTH_TOO_LARGE beyond).  The first
+ * call on a device looks up the array's device address (no allocation);
+ * make that first call before any stream capture.  Every call shares the
+ * array, so calls that can overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+int mb_inclusive_scan_noalloc(mb_executor* exec, const mb_src* in, int op, mb_col out);
 /* vector::exclusive_scan (scan.rs:216; core scan.rs:1180-1234):
  * out[0] = init, out[i] = init op x0 op ... op x(i-1).  `init` points to one
  * host value of the input's vtype. */

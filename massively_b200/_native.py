@@ -65,6 +65,7 @@ def _declare(L: C.CDLL) -> None:
         "mb_copy": (i32, [vp, src, col]),
         "mb_fill": (i32, [vp, vp, col]),
         "mb_inclusive_scan": (i32, [vp, src, i32, col]),
+        "mb_inclusive_scan_noalloc": (i32, [vp, src, i32, col]),
         "mb_exclusive_scan": (i32, [vp, src, i32, vp, col]),
         "mb_reduce": (i32, [vp, src, i32, vp, vp, vp]),
         "mb_copy_where": (i32, [vp, src, i32, src, pcol, pu32, pu32]),

@@ -26,6 +26,8 @@
 // association is a fixed tree inside the tile plus the deterministic fold
 // across tiles, so results are identical run to run.
 
+#include <mutex>
+
 #include "bulk.cuh"
 #include "common.cuh"
 #include "dispatch.cuh"
@@ -456,6 +458,112 @@ int scan_entry(mb_executor* ex, const mb_src* in, int op, bool exclusive, const 
   return set_error(MB_ERR_LAUNCH, "unsupported element type");
 }
 
+// ------------------------------------------------ allocation-free scan ----
+//
+// For callers that cannot allocate device memory during a call.  The
+// look-back scratch (tile ticket, abort word, tile states) lives in this
+// fixed array instead of the executor's pool.  The largest call it admits
+// needs 256 + 32768 tiles * 20 bytes + 64 = 655,680 bytes (2^26 8-byte
+// elements on the register-tiled path); the array is 1 MiB.
+constexpr size_t kNoAllocBytes = 1u << 20;
+constexpr uint64_t kNoAllocMax4 = 1ull << 27;  // 4-byte elements
+constexpr uint64_t kNoAllocMax8 = 1ull << 26;  // 8-byte elements
+
+static __device__ __align__(256) unsigned char g_scan_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the array on `device`, looked up once per device with
+// that device current (host code may not use the symbol itself: on the host
+// it names a host-side stand-in, not device memory).
+int noalloc_scratch(int device, void** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices)
+    return set_error(MB_ERR_LAUNCH, "device ordinal out of range for the allocation-free scan");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[device]) {
+    int prev = 0;
+    MB_CUDA(cudaGetDevice(&prev));
+    if (prev != device) MB_CUDA(cudaSetDevice(device));
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_scan_noalloc_scratch);
+    if (prev != device) cudaSetDevice(prev);
+    if (e != cudaSuccess) return check_cuda(e, "cudaGetSymbolAddress(scan scratch)");
+    g_noalloc_addr[device] = ptr;
+  }
+  *out = g_noalloc_addr[device];
+  return MB_OK;
+}
+
+template <class T>
+int scan_noalloc_run(mb_executor* ex, const mb_src& in, int op, const mb_col& out) {
+  constexpr bool PACKED = sizeof(T) == 4;
+  const uint64_t cap = in.len;
+  if (cap == 0) return MB_OK;
+  if (cap > (sizeof(T) == 4 ? kNoAllocMax4 : kNoAllocMax8))
+    return set_error(MB_ERR_LENGTH_TOO_LARGE,
+                     "allocation-free scan takes at most 2^27 4-byte or 2^26 8-byte elements", cap);
+  const bool plain = src_plain(in, DTypeOf<T>::value) && out.dtype == DTypeOf<T>::value &&
+                     ((uintptr_t)in.data % 16 == 0) && ((uintptr_t)out.data % 16 == 0);
+  const bool smem_path = plain && in.len_dev == nullptr;
+  const uint64_t tile_items = smem_path ? SmemCfg<T>::TILE : ScanCfg<T>::TILE;
+  const uint64_t tiles = (cap + tile_items - 1) / tile_items;
+  const size_t need = 256 + TileState<T, PACKED>::bytes(tiles);
+  if (need > kNoAllocBytes)
+    return set_error(MB_ERR_LENGTH_TOO_LARGE, "allocation-free scan: input too large", cap);
+  void* scratch = nullptr;
+  MB_TRY(noalloc_scratch(ex->device, &scratch));
+  // The array keeps the previous call's contents: clear the ticket, the
+  // abort word and the tile states this call uses.
+  MB_CUDA(cudaMemsetAsync(scratch, 0, need, ex->stream));
+  ScanParams<T> p{};
+  p.op = op;
+  p.exclusive = 0;
+  p.out_dtype = out.dtype;
+  p.init = T(0);
+  p.counter = (uint32_t*)scratch;
+  p.err = DevErr{ex->status_dev, (uint32_t*)scratch + 1};
+  auto st = TileState<T, PACKED>::make((char*)scratch + 256, tiles);
+  const Src s = to_src(in);
+  dim3 grid(grid_for(tiles)), block(kThreads);
+  const size_t smem = SmemCfg<T>::TILE_BYTES;
+#define MB_SCAN_NOALLOC_LAUNCH(OPID)                                                            \
+  do {                                                                                          \
+    if (smem_path) {                                                                            \
+      scan_smem_kernel<T, OPID, PACKED><<<grid, block, smem, ex->stream>>>(                     \
+          (const T*)in.data, (T*)out.data, cap, p, st);                                         \
+    } else if (plain) {                                                                         \
+      scan_kernel<T, OPID, true, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
+    } else {                                                                                    \
+      scan_kernel<T, OPID, false, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
+    }                                                                                           \
+  } while (0)
+  switch (op) {
+    case MB_OP_ADD: MB_SCAN_NOALLOC_LAUNCH(MB_OP_ADD); break;
+    case MB_OP_MIN: MB_SCAN_NOALLOC_LAUNCH(MB_OP_MIN); break;
+    case MB_OP_MAX: MB_SCAN_NOALLOC_LAUNCH(MB_OP_MAX); break;
+    default: MB_SCAN_NOALLOC_LAUNCH(kOpDyn); break;
+  }
+#undef MB_SCAN_NOALLOC_LAUNCH
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int scan_noalloc_entry(mb_executor* ex, const mb_src* in, int op, const mb_col& out) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, in, "input"));
+  MB_TRY(check_col(ex, out, "output"));
+  const int ct = compute_type(in->vtype);
+  if (compute_type(out.dtype) != ct)
+    return set_error(MB_ERR_LAUNCH, "output element type differs from the input's");
+  if (!op_valid_for(op, ct)) return set_error(MB_ERR_LAUNCH, "operator not defined for this type");
+  if (out.len < in->len)
+    return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", in->len, out.len);
+  MB_DISPATCH_CTYPE(ct, scan_noalloc_run, ex, *in, op, out);
+  return set_error(MB_ERR_LAUNCH, "unsupported element type");
+}
+
 }  // namespace
 }  // namespace mb
 
@@ -463,6 +571,10 @@ extern "C" {
 
 int mb_inclusive_scan(mb_executor* ex, const mb_src* in, int op, mb_col out) {
   return mb::scan_entry(ex, in, op, false, nullptr, out);
+}
+
+int mb_inclusive_scan_noalloc(mb_executor* ex, const mb_src* in, int op, mb_col out) {
+  return mb::scan_noalloc_entry(ex, in, op, out);
 }
 
 int mb_exclusive_scan(mb_executor* ex, const mb_src* in, int op, const void* init, mb_col out) {
