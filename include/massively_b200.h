@@ -306,6 +306,15 @@ int mb_sort_by_key(mb_executor* exec, const mb_src* keys, int less, const mb_src
 int mb_reduce_by_key(mb_executor* exec, const mb_src* keys, int key_eq, const mb_src* values,
                      int nvals, const int* ops, const uint64_t* inits, mb_col out_keys,
                      const mb_col* out_values, uint32_t* count_dev, uint32_t* count_host);
+/* reduce_by_key whose runs also break at segment starts (offsets of
+ * `segment_count` segments over the rows).  No counterpart in massively: it
+ * lets a batched caller reduce many independent requests' rows in one
+ * launch without runs merging across request boundaries. */
+int mb_reduce_by_key_segmented(mb_executor* exec, const mb_src* keys, int key_eq,
+                               const mb_src* values, int nvals, const int* ops,
+                               const uint64_t* inits, const uint32_t* offsets,
+                               uint64_t segment_count, mb_col out_keys, const mb_col* out_values,
+                               uint32_t* count_dev, uint32_t* count_host);
 /* vector::inclusive_scan_by_key / exclusive_scan_by_key (by_key.rs:399-560). */
 int mb_inclusive_scan_by_key(mb_executor* exec, const mb_src* keys, int key_eq,
                              const mb_src* values, int op, mb_col out);

@@ -78,6 +78,8 @@ def _declare(L: C.CDLL) -> None:
         "mb_sort_by_key": (i32, [vp, src, i32, src, i32, pcol, pcol]),
         "mb_reduce_by_key": (i32, [vp, src, i32, src, i32, _P(C.c_int), _P(u64), col, pcol,
                                    pu32, pu32]),
+        "mb_reduce_by_key_segmented": (i32, [vp, src, i32, src, i32, _P(C.c_int), _P(u64), vp,
+                                             u64, col, pcol, pu32, pu32]),
         "mb_inclusive_scan_by_key": (i32, [vp, src, i32, src, i32, col]),
         "mb_exclusive_scan_by_key": (i32, [vp, src, i32, src, i32, vp, col]),
         "mb_merge": (i32, [vp, src, src, i32, col]),

@@ -31,6 +31,7 @@
 
 #include <algorithm>
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "lookback.cuh"
 
@@ -48,6 +49,22 @@ constexpr uint32_t kCountMask = 0x3FFFFFFFu;  // status: 2 flag bits + 30 count 
 template <class K, int ENC>
 __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
   return (uint32_t)((enc_bits<K, ENC>(k) >> shift) & (kBins - 1));
+}
+
+// Lanes holding the same 8-bit digit as this lane (digit kBins = no item:
+// matches the other empty lanes only), from one ballot per digit bit plus a
+// validity ballot -- cheaper than match.any under a full SM's load.
+__device__ __forceinline__ unsigned match_digit(uint32_t d) {
+  const bool valid = d < (uint32_t)kBins;
+  const unsigned vb = __ballot_sync(kFull, valid);
+  unsigned m = valid ? vb : ~vb;
+#pragma unroll
+  for (int b = 0; b < kRadixBits; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const unsigned bal = __ballot_sync(kFull, bit);
+    m &= bit ? bal : ~bal;
+  }
+  return m;
 }
 
 // Buffer plan of one sort, filled on the device by the plan kernel.
@@ -359,6 +376,257 @@ size_t onesweep_smem() {
   return sizeof(OnesweepSmem<K, V, THREADS, ITEMS>);
 }
 
+// ------------------------------------------------------- onesweep (TMA) --
+//
+// The same pass for 16-byte-aligned buffers: thread 0 fetches the tile's
+// keys and values into shared memory with cp.async.bulk at CTA start (one
+// DRAM round trip for both, no load instructions, no registers held while
+// they are in flight); ranking reads the keys from shared memory, and the
+// tile is permuted in place through registers.
+
+template <class K, class V, int THREADS, int ITEMS>
+struct OnesweepTmaSmem {
+  static constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int TILE = THREADS * ITEMS;
+  K keys[TILE];                       // 16-byte aligned: bulk-copy target
+  V vals[KEYS_ONLY ? 16 : TILE];
+  uint32_t warp_cnt[WARPS][kBins];
+  uint32_t tile_start[kBins];
+  uint32_t delta[kBins];
+  uint32_t wsum[kBins / 32];
+  uint32_t tile_id;
+  uint32_t pad_;
+  uint64_t bar;
+};
+
+template <class K, int ENC, class V, int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
+    radix_onesweep_tma_kernel(const PassPlan* __restrict__ plan, int pass, uint32_t n,
+                              const uint32_t* __restrict__ digit_offsets,
+                              uint32_t* __restrict__ status, uint32_t* __restrict__ counter,
+                              DevErr err) {
+  using S = OnesweepTmaSmem<K, V, THREADS, ITEMS>;
+  constexpr bool KEYS_ONLY = S::KEYS_ONLY;
+  constexpr int WARPS = S::WARPS;
+  constexpr int TILE = S::TILE;
+  extern __shared__ __align__(128) unsigned char smem_tma[];
+  S& sm = *reinterpret_cast<S*>(smem_tma);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+
+  if (plan->copy_only) {
+    if (pass != 0) return;
+    const K* ik = (const K*)plan->in_k[0];
+    K* ok = (K*)plan->out_k[0];
+    const V* iv = (const V*)plan->in_v[0];
+    V* ov = (V*)plan->out_v[0];
+    for (uint32_t i = blockIdx.x * THREADS + tid; i < n; i += gridDim.x * THREADS) {
+      ok[i] = ik[i];
+      if constexpr (!KEYS_ONLY) ov[i] = iv[i];
+    }
+    return;
+  }
+  if (!plan->active[pass]) return;
+  const K* __restrict__ in_k = (const K*)plan->in_k[pass];
+  K* __restrict__ out_k = (K*)plan->out_k[pass];
+  const V* __restrict__ in_v = (const V*)plan->in_v[pass];
+  V* __restrict__ out_v = (V*)plan->out_v[pass];
+  const int shift = pass * kRadixBits;
+
+  if (tid == 0) {
+    const uint32_t t = atomicAdd(counter, 1u);
+    sm.tile_id = t;
+    mbar_init(&sm.bar, 1);
+    mbar_init_fence();
+    if ((uint64_t)t * TILE + TILE <= n) {
+      constexpr uint32_t kb = TILE * sizeof(K);
+      constexpr uint32_t vb = KEYS_ONLY ? 0 : TILE * sizeof(V);
+      mbar_arrive_expect_tx(&sm.bar, kb + vb);
+      bulk_load(sm.keys, in_k + (uint64_t)t * TILE, kb, &sm.bar);
+      if constexpr (!KEYS_ONLY) bulk_load(sm.vals, in_v + (uint64_t)t * TILE, vb, &sm.bar);
+    }
+  }
+  for (int i = tid; i < WARPS * kBins; i += THREADS) (&sm.warp_cnt[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const uint32_t tile_base = tile * TILE;
+  if (tile_base >= n) return;
+  const uint32_t valid = n - tile_base < (uint32_t)TILE ? n - tile_base : (uint32_t)TILE;
+  if (valid == TILE) {
+    if (!mbar_wait(&sm.bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+  } else {
+    for (uint32_t i = tid; i < valid; i += THREADS) {
+      sm.keys[i] = in_k[tile_base + i];
+      if constexpr (!KEYS_ONLY) sm.vals[i] = in_v[tile_base + i];
+    }
+    __syncthreads();
+  }
+
+  // Warp-striped items: item k of lane l is tile position
+  // warp*32*ITEMS + k*32 + l, so the rounds follow input order.
+  const uint32_t wl = (uint32_t)warp * 32 * ITEMS + lane;
+  auto digit_k = [&](int k) -> uint32_t {
+    const uint32_t li = wl + k * 32;
+    return li < valid ? digit_of<K, ENC>(sm.keys[li], shift) : (uint32_t)kBins;
+  };
+  // Ranking in three phases of independent operations (instead of one
+  // dependent match -> atomic -> shuffle chain per round): all matches, then
+  // the leaders' counter atomics in round order (a warp's atomics on one
+  // address apply in issue order, which keeps the rank stable), then the
+  // broadcasts.
+  unsigned peers[ITEMS];
+  uint32_t rank[ITEMS];
+  uint32_t dpack[(ITEMS + 3) / 4];  // digits, four per register
+  const unsigned lt_mask = (1u << lane) - 1u;
+  if (valid == TILE) {
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t d = digit_of<K, ENC>(sm.keys[wl + k * 32], shift);
+      if (k % 4 == 0) dpack[k / 4] = d;
+      else dpack[k / 4] |= d << (8 * (k % 4));
+      unsigned m = kFull;
+#pragma unroll
+      for (int b = 0; b < kRadixBits; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned bal = __ballot_sync(kFull, bit);
+        m &= bit ? bal : ~bal;
+      }
+      peers[k] = m;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t d = digit_k(k);
+      if (k % 4 == 0) dpack[k / 4] = d & 0xFFu;
+      else dpack[k / 4] |= (d & 0xFFu) << (8 * (k % 4));
+      peers[k] = match_digit(d);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t d = (dpack[k / 4] >> (8 * (k % 4))) & 0xFFu;
+    rank[k] = 0;
+    if (lane == __ffs(peers[k]) - 1 && wl + k * 32 < valid)
+      rank[k] = atomicAdd(&sm.warp_cnt[warp][d], (uint32_t)__popc(peers[k]));
+  }
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k)
+    rank[k] = __shfl_sync(kFull, rank[k], __ffs(peers[k]) - 1) + __popc(peers[k] & lt_mask);
+  K key[ITEMS];
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t li = wl + k * 32;
+    key[k] = li < valid ? sm.keys[li] : K(0);
+  }
+  __syncthreads();  // ranks final; every key of the tile is in registers
+
+  uint32_t tile_count = 0;
+  if (tid < kBins) {
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+      const uint32_t c = sm.warp_cnt[w][tid];
+      sm.warp_cnt[w][tid] = tile_count;
+      tile_count += c;
+    }
+    const uint32_t flag = tile == 0 ? kFlagIncl : kFlagAgg;
+    st_relaxed_u32(status + (uint64_t)tile * kBins + tid, (flag << 30) | tile_count);
+    uint32_t incl = tile_count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, incl, off);
+      if (lane >= off) incl += o;
+    }
+    if (lane == 31) sm.wsum[warp] = incl;
+    sm.tile_start[tid] = incl - tile_count;
+  }
+  __syncthreads();
+  if (tid < kBins) {
+    uint32_t add = 0;
+    for (int w = 0; w < warp; ++w) add += sm.wsum[w];
+    sm.tile_start[tid] += add;
+  }
+  __syncthreads();
+
+  // Keys to their tile-sorted positions (in place: all were read above).
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t d = (dpack[k / 4] >> (8 * (k % 4))) & 0xFFu;
+    rank[k] += sm.tile_start[d] + sm.warp_cnt[warp][d];
+  }
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k)
+    if (wl + k * 32 < valid) sm.keys[rank[k]] = key[k];
+  V val[KEYS_ONLY ? 1 : ITEMS];
+  if constexpr (!KEYS_ONLY) {
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t li = wl + k * 32;
+      val[k] = li < valid ? sm.vals[li] : V(0);
+    }
+  }
+
+  // Decoupled look-back, one digit per thread, eight predecessors per step.
+  if (tid < kBins) {
+    uint32_t excl = 0;
+    if (tile > 0) {
+      constexpr int kBatch = 8;
+      SpinGuard guard(err.abort);
+      int64_t t = (int64_t)tile - 1;
+      bool failed = false, done = false;
+      while (!done) {
+        uint32_t w[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j)
+          w[j] = t - j >= 0 ? ld_relaxed_u32(status + (uint64_t)(t - j) * kBins + tid)
+                            : (kFlagIncl << 30);
+        int used = 0;
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+          if (done || used < j) break;
+          const uint32_t f = w[j] >> 30;
+          if (f == kFlagNone) break;
+          excl += w[j] & kCountMask;
+          ++used;
+          if (f == kFlagIncl) done = true;
+        }
+        t -= used;
+        if (!done && used < kBatch && guard.expired()) { failed = true; break; }
+      }
+      if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+      st_relaxed_u32(status + (uint64_t)tile * kBins + tid,
+                     (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
+    }
+    sm.delta[tid] = digit_offsets[pass * kBins + tid] + excl - sm.tile_start[tid];
+  }
+  if constexpr (!KEYS_ONLY) {
+    __syncthreads();  // every original value is in registers
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k)
+      if (wl + k * 32 < valid) sm.vals[rank[k]] = val[k];
+  }
+  __syncthreads();
+
+  // Write-out, fully unrolled so the shared-memory reads of all ITEMS
+  // positions are in flight together.
+#pragma unroll
+  for (int r = 0; r < ITEMS; ++r) {
+    const uint32_t i = (uint32_t)r * THREADS + tid;
+    if (i >= valid) break;
+    const K kk = sm.keys[i];
+    const uint32_t d = digit_of<K, ENC>(kk, shift);
+    const uint32_t o = sm.delta[d] + i;
+    if (o >= n) {  // only reachable after a failed look-back
+      raise_device_error(err, MB_DEV_ERR_BOUNDS);
+      continue;
+    }
+    __stcs(out_k + o, kk);
+    if constexpr (!KEYS_ONLY) __stcs(out_v + o, sm.vals[i]);
+  }
+}
+
 // Tile configurations of the onesweep kernel (MB_TUNE_RADIX).
 struct RadixCfg {
   int threads, items;
@@ -411,10 +679,23 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   radix_plan_kernel<<<1, kBins, 0, ex->stream>>>(hist, PASSES, n, plan, in_k, final_k, tmp_k,
                                                  in_v, out_v, tmp_v);
   MB_CUDA(cudaGetLastError());
+  const DevErr err{ex->status_dev, counters + 32};
+  const bool aligned = (uintptr_t)in_k % 16 == 0 && (uintptr_t)final_k % 16 == 0 &&
+                       (KEYS_ONLY || ((uintptr_t)in_v % 16 == 0 && (uintptr_t)out_v % 16 == 0));
+  if (aligned) {
+    const size_t smem = sizeof(OnesweepTmaSmem<K, V, THREADS, ITEMS>);
+    auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS>;
+    MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int p = 0; p < PASSES; ++p) {
+      kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
+          plan, p, (uint32_t)n, hist, status + (size_t)p * tiles * kBins, counters + p, err);
+      MB_CUDA(cudaGetLastError());
+    }
+    return MB_OK;
+  }
   const size_t smem = onesweep_smem<K, V, THREADS, ITEMS>();
   auto kern = radix_onesweep_kernel<K, ENC, V, THREADS, ITEMS>;
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const DevErr err{ex->status_dev, counters + 32};
   for (int p = 0; p < PASSES; ++p) {
     kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
         plan, p, n, hist, status + (size_t)p * tiles * kBins, counters + p, err);

@@ -168,10 +168,26 @@ __global__ void __launch_bounds__(kThreads)
       if (!h) h = !key_eq(p.keys.vtype, src_load_bits(p.keys, i - 1), src_load_bits(p.keys, i));
       if (h) atomicOr(&s_bits[(i - tb) >> 5], 1u << ((i - tb) & 31));
     }
-    if (tid == 0)
-      s_head_te = te < n ? !key_eq(p.keys.vtype, src_load_bits(p.keys, te - 1),
-                                   src_load_bits(p.keys, te))
-                         : 1u;
+    if (tid == 0) {
+      uint32_t h = te < n ? !key_eq(p.keys.vtype, src_load_bits(p.keys, te - 1),
+                                    src_load_bits(p.keys, te))
+                          : 1u;
+      if (p.offsets) {  // segment starts are run heads too
+        const uint64_t cnt = p.nseg + 1;
+        s_seg[1] = lower_bound_u32(p.offsets, cnt, tb);
+        s_seg[2] = min(lower_bound_u32(p.offsets, cnt, te), p.nseg);
+        const uint64_t at = lower_bound_u32(p.offsets, cnt, te);
+        if (te < n && at < p.nseg && p.offsets[at] == te) h = 1u;
+      }
+      s_head_te = h;
+    }
+    if (p.offsets) {
+      __syncthreads();
+      for (uint64_t s = s_seg[1] + tid; s < s_seg[2]; s += kThreads) {
+        const uint64_t start = p.offsets[s];
+        if (start >= tb && start < te) atomicOr(&s_bits[(start - tb) >> 5], 1u << ((start - tb) & 31));
+      }
+    }
   }
   __syncthreads();
 
@@ -704,6 +720,15 @@ int mb_exclusive_scan_by_key(mb_executor* ex, const mb_src* keys, int key_eq,
 int mb_reduce_by_key(mb_executor* ex, const mb_src* keys, int key_eq, const mb_src* values,
                      int nvals, const int* ops, const uint64_t* inits, mb_col out_keys,
                      const mb_col* out_values, uint32_t* count_dev, uint32_t* count_host) {
+  return mb_reduce_by_key_segmented(ex, keys, key_eq, values, nvals, ops, inits, nullptr, 0,
+                                    out_keys, out_values, count_dev, count_host);
+}
+
+int mb_reduce_by_key_segmented(mb_executor* ex, const mb_src* keys, int key_eq,
+                               const mb_src* values, int nvals, const int* ops,
+                               const uint64_t* inits, const uint32_t* offsets,
+                               uint64_t segment_count, mb_col out_keys, const mb_col* out_values,
+                               uint32_t* count_dev, uint32_t* count_host) {
   MB_TRY(check_exec(ex));
   MB_TRY(check_src(ex, keys, "keys"));
   MB_TRY(check_col(ex, out_keys, "key output"));
@@ -727,7 +752,8 @@ int mb_reduce_by_key(mb_executor* ex, const mb_src* keys, int key_eq, const mb_s
   } else {
     for (int c = 0; c < nvals; ++c) {
       MB_TRY(seg_entry(ex, &values[c], ops[c], kReduce, &inits[c], out_values[c].data,
-                       out_values[c].dtype, nullptr, 0, keys, c == 0 ? out_keys.data : nullptr,
+                       out_values[c].dtype, offsets, segment_count, keys,
+                       c == 0 ? out_keys.data : nullptr,
                        (int)dtype_size(out_keys.dtype), c == 0 ? count_dev : nullptr));
     }
   }

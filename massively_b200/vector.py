@@ -403,6 +403,28 @@ def reduce_by_key(exec: Executor, keys, values, equal, init, op):
     return kout, _wrap(values, vout)
 
 
+def reduce_by_key_segmented(exec: Executor, keys, values, equal, init, op, offsets: DeviceVec):
+    """reduce_by_key whose runs also break at the segment starts given by
+    `offsets` (segment_count + 1 entries): many independent requests' rows
+    reduce in one launch (no massively counterpart; the batched loop uses it)."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks = lower(exec, keys, keep)
+    vs, nv = _srcs(exec, values, keep)
+    ids, bits = _ops_inits(values, op, init)
+    cnt = _count_buffer(exec)
+    kout = exec.alloc(_dtype(keys), n).with_len_dev(cnt)
+    vout = _out_like(exec, values, n, cnt)
+    check(_L().mb_reduce_by_key_segmented(
+        exec.handle, C.byref(ks), O.pred2(equal).id, vs, nv, ids, bits,
+        C.c_void_p(offsets.data_ptr()), len(offsets) - 1, kout.to_col(), _cols(vout), _p32(cnt),
+        None))
+    return kout, _wrap(values, vout)
+
+
 def inclusive_scan_by_key(exec: Executor, keys, values, equal, op):
     """vector::inclusive_scan_by_key (by_key.rs:399)."""
     _check_owner(exec, keys, values)
