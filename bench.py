@@ -33,6 +33,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# torch and the kernels' scratch share the device's stream-ordered pool
+# (set before torch first touches CUDA; see massively_b200/__init__.py).
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "backend:cudaMallocAsync")
 
 FALLBACK_HBM_GBS = 6650.0
 

@@ -40,7 +40,8 @@ namespace {
 
 constexpr int kRadixBits = 8;
 constexpr int kBins = 1 << kRadixBits;
-constexpr int kHistThreads = 256;
+constexpr int kHistThreads = 512;
+constexpr int kHistUnroll = 4;  // 16-byte vectors per lane per chunk
 constexpr uint32_t kCountMask = 0x3FFFFFFFu;  // status: 2 flag bits + 30 count bits
 
 // Keys travel as their raw unsigned bits (K = uint32_t / uint64_t) and are
@@ -80,33 +81,77 @@ struct PassPlan {
 
 // ----------------------------------------------------------- histogram --
 
+// All passes' digit counts in one read of the keys.  Each warp takes chunks
+// of kHistUnroll x 32 16-byte vectors (all loads issued before any count),
+// and counts into its own sub-histogram (COPIES per block, so warps of one
+// block rarely contend on a bin).  Digit positions where every key of the
+// chunk agrees (the high bytes of small keys, constant columns) are found
+// with one OR-reduction per chunk and counted by one add, instead of 32-way
+// conflicting atomics.  Keys that are not 16-byte aligned, and the tail after
+// the last full chunk, go one key per thread.
 template <class K, int ENC, int PASSES>
-__global__ void __launch_bounds__(kHistThreads)
+__global__ void __launch_bounds__(kHistThreads, 2)
     radix_histogram_kernel(const K* __restrict__ keys, uint64_t n, uint32_t* __restrict__ hist) {
-  __shared__ uint32_t sh[PASSES][kBins];
-  for (int i = threadIdx.x; i < PASSES * kBins; i += kHistThreads) (&sh[0][0])[i] = 0;
+  constexpr int COPIES = 16 / PASSES;
+  constexpr int KPV = 16 / (int)sizeof(K);      // keys per 16-byte vector
+  constexpr int KPL = KPV * kHistUnroll;        // keys per lane per chunk
+  constexpr uint64_t KPW = 32ull * KPL;         // keys per warp chunk
+  __shared__ uint32_t sh[COPIES][PASSES][kBins];
+  for (int i = threadIdx.x; i < COPIES * PASSES * kBins; i += kHistThreads)
+    (&sh[0][0][0])[i] = 0;
   __syncthreads();
-  const uint64_t step = (uint64_t)gridDim.x * kHistThreads;
-  for (uint64_t i = blockIdx.x * (uint64_t)kHistThreads + threadIdx.x; i - threadIdx.x < n;
-       i += step) {
-    const bool valid = i < n;
-    const K u = valid ? enc_bits<K, ENC>(__ldcs(keys + i)) : (K)0;
+  uint32_t(*h)[kBins] = sh[(threadIdx.x >> 5) % COPIES];
+  const uint32_t lane = lane_id();
+  const uint64_t warps = (uint64_t)gridDim.x * (kHistThreads / 32);
+  const uint64_t gw = (uint64_t)blockIdx.x * (kHistThreads / 32) + (threadIdx.x >> 5);
+  const uint64_t chunks = ((uintptr_t)keys & 15) == 0 ? n / KPW : 0;
+  for (uint64_t c = gw; c < chunks; c += warps) {
+    const uint4* src = reinterpret_cast<const uint4*>(keys + c * KPW);
+    uint4 v[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) v[u] = __ldcs(src + u * 32 + lane);
+    K k[KPL];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) {
+      const K* kv = reinterpret_cast<const K*>(&v[u]);
+#pragma unroll
+      for (int j = 0; j < KPV; ++j) k[u * KPV + j] = enc_bits<K, ENC>(kv[j]);
+    }
+    K any = 0, all = ~(K)0;
+#pragma unroll
+    for (int j = 0; j < KPL; ++j) {
+      any |= k[j];
+      all &= k[j];
+    }
+    const K ref = __shfl_sync(kFull, k[0], 0);
+    const K diff = (any ^ all) | (k[0] ^ ref);
+    K wdiff = (K)__reduce_or_sync(kFull, (uint32_t)diff);
+    if constexpr (sizeof(K) == 8)
+      wdiff |= (K)__reduce_or_sync(kFull, (uint32_t)((uint64_t)diff >> 32)) << 32;
 #pragma unroll
     for (int p = 0; p < PASSES; ++p) {
-      const uint32_t d = (uint32_t)((u >> (p * kRadixBits)) & (kBins - 1));
-      // Whole warp on one digit (skewed keys): one add of the warp count.
-      const uint32_t d0 = __shfl_sync(kFull, d, 0);
-      const unsigned vmask = __ballot_sync(kFull, valid);
-      if (__all_sync(kFull, d == d0 || !valid)) {
-        if (lane_id() == 0 && vmask) atomicAdd(&sh[p][d0], (uint32_t)__popc(vmask));
-      } else if (valid) {
-        atomicAdd(&sh[p][d], 1u);
+      const int s = p * kRadixBits;
+      if (((wdiff >> s) & (kBins - 1)) == 0) {  // warp-uniform
+        if (lane == 0) atomicAdd(&h[p][(uint32_t)(ref >> s) & (kBins - 1)], (uint32_t)KPW);
+      } else {
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) atomicAdd(&h[p][(uint32_t)(k[j] >> s) & (kBins - 1)], 1u);
       }
     }
   }
+  const uint64_t stride = (uint64_t)gridDim.x * kHistThreads;
+  for (uint64_t i = chunks * KPW + (uint64_t)blockIdx.x * kHistThreads + threadIdx.x; i < n;
+       i += stride) {
+    const K u = enc_bits<K, ENC>(__ldcs(keys + i));
+#pragma unroll
+    for (int p = 0; p < PASSES; ++p)
+      atomicAdd(&h[p][(uint32_t)(u >> (p * kRadixBits)) & (kBins - 1)], 1u);
+  }
   __syncthreads();
   for (int i = threadIdx.x; i < PASSES * kBins; i += kHistThreads) {
-    uint32_t c = (&sh[0][0])[i];
+    uint32_t c = 0;
+#pragma unroll
+    for (int cp = 0; cp < COPIES; ++cp) c += (&sh[cp][0][0])[i];
     if (c) atomicAdd(hist + i, c);
   }
 }
@@ -383,15 +428,28 @@ size_t onesweep_smem() {
 // DRAM round trip for both, no load instructions, no registers held while
 // they are in flight); ranking reads the keys from shared memory, and the
 // tile is permuted in place through registers.
+//
+// Ranking, per warp round of 32 keys: the lanes holding the same digit
+// (peers) come from a per-warp table of 256 lane masks in shared memory --
+// each lane ORs its bit into its digit's word and reads the word back --
+// instead of eight ballots per key.  NT tables are used in turn: with one,
+// a round needs three warp barriers (set, read, clear); with three, a
+// round's words are cleared two rounds later, so one barrier per round
+// suffices.  Then the lowest peer of each round adds the peer count to the
+// warp's per-digit counter, in round order (one warp's atomics on one
+// address apply in issue order, which keeps the ranks stable), and
+// broadcasts the old count to its peers.
 
-template <class K, class V, int THREADS, int ITEMS>
+template <class K, class V, int THREADS, int ITEMS, int NT>
 struct OnesweepTmaSmem {
   static constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
   static constexpr int WARPS = THREADS / 32;
   static constexpr int TILE = THREADS * ITEMS;
   K keys[TILE];                       // 16-byte aligned: bulk-copy target
   V vals[KEYS_ONLY ? 16 : TILE];
-  uint32_t warp_cnt[WARPS][kBins];
+  // Slot kBins takes the empty items of a partial tile.
+  uint32_t mask[NT][WARPS][kBins + 1];
+  uint32_t warp_cnt[WARPS][kBins + 1];
   uint32_t tile_start[kBins];
   uint32_t delta[kBins];
   uint32_t wsum[kBins / 32];
@@ -400,129 +458,70 @@ struct OnesweepTmaSmem {
   uint64_t bar;
 };
 
-template <class K, int ENC, class V, int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
-    radix_onesweep_tma_kernel(const PassPlan* __restrict__ plan, int pass, uint32_t n,
-                              const uint32_t* __restrict__ digit_offsets,
-                              uint32_t* __restrict__ status, uint32_t* __restrict__ counter,
-                              DevErr err) {
-  using S = OnesweepTmaSmem<K, V, THREADS, ITEMS>;
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool FULL>
+__device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>& sm,
+                                              const uint32_t tile, const uint32_t valid,
+                                              const int pass, const uint32_t n,
+                                              const uint32_t* __restrict__ digit_offsets,
+                                              uint32_t* __restrict__ status, const DevErr err,
+                                              K* __restrict__ out_k, V* __restrict__ out_v) {
+  using S = OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>;
   constexpr bool KEYS_ONLY = S::KEYS_ONLY;
   constexpr int WARPS = S::WARPS;
-  constexpr int TILE = S::TILE;
-  extern __shared__ __align__(128) unsigned char smem_tma[];
-  S& sm = *reinterpret_cast<S*>(smem_tma);
-
+  static_assert(S::TILE <= 65536, "tile positions must fit 16 bits");
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const int lane = tid & 31;
-
-  if (plan->copy_only) {
-    if (pass != 0) return;
-    const K* ik = (const K*)plan->in_k[0];
-    K* ok = (K*)plan->out_k[0];
-    const V* iv = (const V*)plan->in_v[0];
-    V* ov = (V*)plan->out_v[0];
-    for (uint32_t i = blockIdx.x * THREADS + tid; i < n; i += gridDim.x * THREADS) {
-      ok[i] = ik[i];
-      if constexpr (!KEYS_ONLY) ov[i] = iv[i];
-    }
-    return;
-  }
-  if (!plan->active[pass]) return;
-  const K* __restrict__ in_k = (const K*)plan->in_k[pass];
-  K* __restrict__ out_k = (K*)plan->out_k[pass];
-  const V* __restrict__ in_v = (const V*)plan->in_v[pass];
-  V* __restrict__ out_v = (V*)plan->out_v[pass];
   const int shift = pass * kRadixBits;
-
-  if (tid == 0) {
-    const uint32_t t = atomicAdd(counter, 1u);
-    sm.tile_id = t;
-    mbar_init(&sm.bar, 1);
-    mbar_init_fence();
-    if ((uint64_t)t * TILE + TILE <= n) {
-      constexpr uint32_t kb = TILE * sizeof(K);
-      constexpr uint32_t vb = KEYS_ONLY ? 0 : TILE * sizeof(V);
-      mbar_arrive_expect_tx(&sm.bar, kb + vb);
-      bulk_load(sm.keys, in_k + (uint64_t)t * TILE, kb, &sm.bar);
-      if constexpr (!KEYS_ONLY) bulk_load(sm.vals, in_v + (uint64_t)t * TILE, vb, &sm.bar);
-    }
-  }
-  for (int i = tid; i < WARPS * kBins; i += THREADS) (&sm.warp_cnt[0][0])[i] = 0;
-  __syncthreads();
-  const uint32_t tile = sm.tile_id;
-  const uint32_t tile_base = tile * TILE;
-  if (tile_base >= n) return;
-  const uint32_t valid = n - tile_base < (uint32_t)TILE ? n - tile_base : (uint32_t)TILE;
-  if (valid == TILE) {
-    if (!mbar_wait(&sm.bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-  } else {
-    for (uint32_t i = tid; i < valid; i += THREADS) {
-      sm.keys[i] = in_k[tile_base + i];
-      if constexpr (!KEYS_ONLY) sm.vals[i] = in_v[tile_base + i];
-    }
-    __syncthreads();
-  }
-
   // Warp-striped items: item k of lane l is tile position
   // warp*32*ITEMS + k*32 + l, so the rounds follow input order.
   const uint32_t wl = (uint32_t)warp * 32 * ITEMS + lane;
-  auto digit_k = [&](int k) -> uint32_t {
+  const uint32_t below_me = (1u << lane) - 1u;
+  const uint32_t me = 1u << lane;
+
+  uint32_t peers[ITEMS];
+  uint32_t rd[ITEMS];  // digit << 16, then | rank
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
     const uint32_t li = wl + k * 32;
-    return li < valid ? digit_of<K, ENC>(sm.keys[li], shift) : (uint32_t)kBins;
-  };
-  // Ranking in three phases of independent operations (instead of one
-  // dependent match -> atomic -> shuffle chain per round): all matches, then
-  // the leaders' counter atomics in round order (a warp's atomics on one
-  // address apply in issue order, which keeps the rank stable), then the
-  // broadcasts.
-  unsigned peers[ITEMS];
-  uint32_t rank[ITEMS];
-  uint32_t dpack[(ITEMS + 3) / 4];  // digits, four per register
-  const unsigned lt_mask = (1u << lane) - 1u;
-  if (valid == TILE) {
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      const uint32_t d = digit_of<K, ENC>(sm.keys[wl + k * 32], shift);
-      if (k % 4 == 0) dpack[k / 4] = d;
-      else dpack[k / 4] |= d << (8 * (k % 4));
-      unsigned m = kFull;
-#pragma unroll
-      for (int b = 0; b < kRadixBits; ++b) {
-        const bool bit = (d >> b) & 1u;
-        const unsigned bal = __ballot_sync(kFull, bit);
-        m &= bit ? bal : ~bal;
-      }
-      peers[k] = m;
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      const uint32_t d = digit_k(k);
-      if (k % 4 == 0) dpack[k / 4] = d & 0xFFu;
-      else dpack[k / 4] |= (d & 0xFFu) << (8 * (k % 4));
-      peers[k] = match_digit(d);
+    const uint32_t d = (FULL || li < valid) ? digit_of<K, ENC>(sm.keys[li], shift) : (uint32_t)kBins;
+    rd[k] = d << 16;
+    uint32_t* m = sm.mask[k % NT][warp];
+    atomicOr(&m[d], me);
+    __syncwarp();
+    peers[k] = m[d];
+    if constexpr (NT == 1) {
+      __syncwarp();
+      m[d] = 0;
+      __syncwarp();
+    } else {
+      static_assert(NT >= 3, "a round's words are cleared two rounds before reuse");
+      if (k > 0) sm.mask[(k - 1) % NT][warp][rd[k - 1] >> 16] = 0;
     }
   }
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t d = (dpack[k / 4] >> (8 * (k % 4))) & 0xFFu;
-    rank[k] = 0;
-    if (lane == __ffs(peers[k]) - 1 && wl + k * 32 < valid)
-      rank[k] = atomicAdd(&sm.warp_cnt[warp][d], (uint32_t)__popc(peers[k]));
+    uint32_t base = 0;
+    if ((peers[k] & below_me) == 0)
+      base = atomicAdd(&sm.warp_cnt[warp][rd[k] >> 16], (uint32_t)__popc(peers[k]));
+    rd[k] |= base;
   }
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k)
-    rank[k] = __shfl_sync(kFull, rank[k], __ffs(peers[k]) - 1) + __popc(peers[k] & lt_mask);
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t base = __shfl_sync(kFull, rd[k] & 0xFFFFu, __ffs(peers[k]) - 1);
+    rd[k] = (rd[k] & 0xFFFF0000u) | (base + __popc(peers[k] & below_me));
+  }
   K key[ITEMS];
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
     const uint32_t li = wl + k * 32;
-    key[k] = li < valid ? sm.keys[li] : K(0);
+    key[k] = (FULL || li < valid) ? sm.keys[li] : K(0);
   }
-  __syncthreads();  // ranks final; every key of the tile is in registers
+  __syncthreads();  // counts final; every key of the tile is in registers
 
+  // Per digit: the warps' counts to exclusive offsets, the tile's count
+  // (published at once for the successors' look-back), and the tile-wide
+  // exclusive offsets.
   uint32_t tile_count = 0;
   if (tid < kBins) {
 #pragma unroll
@@ -553,18 +552,18 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
   // Keys to their tile-sorted positions (in place: all were read above).
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t d = (dpack[k / 4] >> (8 * (k % 4))) & 0xFFu;
-    rank[k] += sm.tile_start[d] + sm.warp_cnt[warp][d];
+    const uint32_t d = rd[k] >> 16;
+    rd[k] = (rd[k] & 0xFFFFu) + sm.tile_start[d & (kBins - 1)] + sm.warp_cnt[warp][d];
   }
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k)
-    if (wl + k * 32 < valid) sm.keys[rank[k]] = key[k];
+    if (FULL || wl + k * 32 < valid) sm.keys[rd[k]] = key[k];
   V val[KEYS_ONLY ? 1 : ITEMS];
   if constexpr (!KEYS_ONLY) {
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
       const uint32_t li = wl + k * 32;
-      val[k] = li < valid ? sm.vals[li] : V(0);
+      val[k] = (FULL || li < valid) ? sm.vals[li] : V(0);
     }
   }
 
@@ -605,7 +604,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
     __syncthreads();  // every original value is in registers
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k)
-      if (wl + k * 32 < valid) sm.vals[rank[k]] = val[k];
+      if (FULL || wl + k * 32 < valid) sm.vals[rd[k]] = val[k];
   }
   __syncthreads();
 
@@ -614,10 +613,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
 #pragma unroll
   for (int r = 0; r < ITEMS; ++r) {
     const uint32_t i = (uint32_t)r * THREADS + tid;
-    if (i >= valid) break;
+    if (!FULL && i >= valid) break;
     const K kk = sm.keys[i];
-    const uint32_t d = digit_of<K, ENC>(kk, shift);
-    const uint32_t o = sm.delta[d] + i;
+    const uint32_t o = sm.delta[digit_of<K, ENC>(kk, shift)] + i;
     if (o >= n) {  // only reachable after a failed look-back
       raise_device_error(err, MB_DEV_ERR_BOUNDS);
       continue;
@@ -627,19 +625,90 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
   }
 }
 
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT>
+__global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THREADS >= 384 ? 2 : 4) : 3)
+    radix_onesweep_tma_kernel(const PassPlan* __restrict__ plan, int pass, uint32_t n,
+                              const uint32_t* __restrict__ digit_offsets,
+                              uint32_t* __restrict__ status, uint32_t* __restrict__ counter,
+                              DevErr err) {
+  using S = OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>;
+  constexpr bool KEYS_ONLY = S::KEYS_ONLY;
+  constexpr int WARPS = S::WARPS;
+  constexpr int TILE = S::TILE;
+  extern __shared__ __align__(128) unsigned char smem_tma[];
+  S& sm = *reinterpret_cast<S*>(smem_tma);
+  const int tid = threadIdx.x;
+
+  if (plan->copy_only) {
+    if (pass != 0) return;
+    const K* ik = (const K*)plan->in_k[0];
+    K* ok = (K*)plan->out_k[0];
+    const V* iv = (const V*)plan->in_v[0];
+    V* ov = (V*)plan->out_v[0];
+    for (uint32_t i = blockIdx.x * THREADS + tid; i < n; i += gridDim.x * THREADS) {
+      ok[i] = ik[i];
+      if constexpr (!KEYS_ONLY) ov[i] = iv[i];
+    }
+    return;
+  }
+  if (!plan->active[pass]) return;
+  const K* __restrict__ in_k = (const K*)plan->in_k[pass];
+  const V* __restrict__ in_v = (const V*)plan->in_v[pass];
+
+  if (tid == 0) {
+    const uint32_t t = atomicAdd(counter, 1u);
+    sm.tile_id = t;
+    mbar_init(&sm.bar, 1);
+    mbar_init_fence();
+    if ((uint64_t)t * TILE + TILE <= n) {
+      constexpr uint32_t kb = TILE * sizeof(K);
+      constexpr uint32_t vb = KEYS_ONLY ? 0 : TILE * sizeof(V);
+      mbar_arrive_expect_tx(&sm.bar, kb + vb);
+      bulk_load(sm.keys, in_k + (uint64_t)t * TILE, kb, &sm.bar);
+      if constexpr (!KEYS_ONLY) bulk_load(sm.vals, in_v + (uint64_t)t * TILE, vb, &sm.bar);
+    }
+  }
+  for (int i = tid; i < (NT + 1) * WARPS * (kBins + 1); i += THREADS)
+    (&sm.mask[0][0][0])[i] = 0;  // mask tables and warp_cnt (adjacent)
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const uint32_t tile_base = tile * TILE;
+  if (tile_base >= n) return;
+  const uint32_t valid = n - tile_base < (uint32_t)TILE ? n - tile_base : (uint32_t)TILE;
+  K* out_k = (K*)plan->out_k[pass];
+  V* out_v = (V*)plan->out_v[pass];
+  if (valid == TILE) {
+    if (!mbar_wait(&sm.bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, true>(sm, tile, valid, pass, n, digit_offsets,
+                                                   status, err, out_k, out_v);
+  } else {
+    for (uint32_t i = tid; i < valid; i += THREADS) {
+      sm.keys[i] = in_k[tile_base + i];
+      if constexpr (!KEYS_ONLY) sm.vals[i] = in_v[tile_base + i];
+    }
+    __syncthreads();
+    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, false>(sm, tile, valid, pass, n, digit_offsets,
+                                                    status, err, out_k, out_v);
+  }
+}
+
 // Tile configurations of the onesweep kernel (MB_TUNE_RADIX).
 struct RadixCfg {
   int threads, items;
   const char* text;
 };
 constexpr RadixCfg kRadixCfgs[] = {
-    {256, 16, "onesweep 256 threads x 16 keys (4096-key tiles)"},
-    {256, 24, "onesweep 256 threads x 24 keys (6144-key tiles)"},
-    {512, 16, "onesweep 512 threads x 16 keys (8192-key tiles)"},
+    {256, 16, "onesweep 256 threads x 16 keys, one peer-mask table (three warp barriers per round)"},
+    {256, 16, "onesweep 256 threads x 16 keys, three peer-mask tables (one warp barrier per round)"},
+    {512, 16, "onesweep 512 threads x 16 keys (8192-key tiles), one peer-mask table"},
+    {256, 12, "onesweep 256 threads x 12 keys (3072-key tiles), three peer-mask tables"},
+    {1024, 16, "onesweep 1024 threads x 16 keys (16384-key tiles), one peer-mask table"},
+    {384, 16, "onesweep 384 threads x 16 keys (6144-key tiles), one peer-mask table"},
 };
-constexpr int kRadixDefault = 0;
+constexpr int kRadixDefault = 0;    // 64-bit keys or values
+constexpr int kRadixDefault32 = 2;  // 32-bit keys, values of at most 32 bits
 
-template <class K, int ENC, class V, int THREADS, int ITEMS>
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT = 1>
 int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v,
                       uint64_t n) {
   constexpr int PASSES = (int)sizeof(K);
@@ -671,8 +740,10 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
 
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ex->device);
+  // Each block counts at least one chunk per warp (16 keys per thread); at
+  // most two blocks per SM stay resident.
   const uint64_t hist_blocks = std::min<uint64_t>((n + kHistThreads * 16 - 1) / (kHistThreads * 16),
-                                                  (uint64_t)sms * 4);
+                                                  (uint64_t)sms * 2);
   radix_histogram_kernel<K, ENC, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks), kHistThreads,
                                       0, ex->stream>>>(in_k, n, hist);
   MB_CUDA(cudaGetLastError());
@@ -683,8 +754,8 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   const bool aligned = (uintptr_t)in_k % 16 == 0 && (uintptr_t)final_k % 16 == 0 &&
                        (KEYS_ONLY || ((uintptr_t)in_v % 16 == 0 && (uintptr_t)out_v % 16 == 0));
   if (aligned) {
-    const size_t smem = sizeof(OnesweepTmaSmem<K, V, THREADS, ITEMS>);
-    auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS>;
+    const size_t smem = sizeof(OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>);
+    auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS, NT>;
     MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int p = 0; p < PASSES; ++p) {
       kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
@@ -708,11 +779,14 @@ template <class K, int ENC, class V>
 int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v, uint64_t n) {
   if (n == 0) return MB_OK;
   int cfg = ex->tune[MB_TUNE_RADIX];
-  if (cfg < 0) cfg = kRadixDefault;
+  if (cfg < 0) cfg = (sizeof(K) == 4 && sizeof(V) <= 4) ? kRadixDefault32 : kRadixDefault;
   switch (cfg) {
-    case 1: return onesweep_sort_cfg<K, ENC, V, 256, 24>(ex, in_k, in_v, out_k, out_v, n);
-    case 2: return onesweep_sort_cfg<K, ENC, V, 512, 16>(ex, in_k, in_v, out_k, out_v, n);
-    default: return onesweep_sort_cfg<K, ENC, V, 256, 16>(ex, in_k, in_v, out_k, out_v, n);
+    case 1: return onesweep_sort_cfg<K, ENC, V, 256, 16, 3>(ex, in_k, in_v, out_k, out_v, n);
+    case 2: return onesweep_sort_cfg<K, ENC, V, 512, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
+    case 3: return onesweep_sort_cfg<K, ENC, V, 256, 12, 3>(ex, in_k, in_v, out_k, out_v, n);
+    case 4: return onesweep_sort_cfg<K, ENC, V, 1024, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
+    case 5: return onesweep_sort_cfg<K, ENC, V, 384, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
+    default: return onesweep_sort_cfg<K, ENC, V, 256, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
   }
 }
 

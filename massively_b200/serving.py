@@ -45,8 +45,10 @@ class Request:
     done: float = math.nan  # completion, seconds after the trace start
 
     def bytes_needed(self) -> int:
-        # inputs + outputs on the device
-        return {SORT: 16, SCAN: 8, RBK: 24}[self.kind] * self.n
+        # inputs + outputs + the kernels' scratch on the device (the sort's
+        # ping-pong buffers and look-back states, the run-count scratch of
+        # reduce_by_key)
+        return {SORT: 26, SCAN: 9, RBK: 28}[self.kind] * self.n
 
 
 def make_trace(rate: float = 20_000.0, duration: float = 1.0, lo_log2: int = 10,

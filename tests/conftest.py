@@ -3,6 +3,10 @@ import sys
 
 import pytest
 
+# One stream-ordered pool for torch and the kernels' scratch (set before
+# torch first touches CUDA).
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "backend:cudaMallocAsync")
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)

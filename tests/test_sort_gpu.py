@@ -161,3 +161,26 @@ def test_large_pairs(ex):
     want = np.argsort(keys, kind="stable").astype(np.uint32)
     np.testing.assert_array_equal(ex.to_host(sv), want)
     np.testing.assert_array_equal(ex.to_host(sk), keys[want])
+
+
+@pytest.mark.parametrize("n", [1, 4095, 4096, 65_537, 1 << 20])
+@pytest.mark.parametrize("keyspace", ["full", "16bit", "const"])
+def test_every_radix_config_bit_exact(n, keyspace):
+    """Each onesweep configuration the autotuner may choose sorts the same."""
+    from massively_b200 import tune, vector
+    ex = executor()
+    keys = seeded(np.uint32, n, seed=n + 5)
+    if keyspace == "16bit":
+        keys = keys & np.uint32(0xFFFF)
+    elif keyspace == "const":
+        keys = np.full(n, 3, np.uint32)
+    vals = _perm_values(n)
+    want = orc.radix_perm([keys])
+    for cfg in range(len(tune.configs("radix"))):
+        tune.set_config(ex, "radix", cfg)
+        for kdt in (np.uint32, np.float32):
+            k = keys.view(kdt)
+            sk, sv = vector.radix_sort_pairs(ex, ex.to_device(k), ex.to_device(vals))
+            w = want if kdt == np.uint32 else orc.radix_perm([k])
+            np.testing.assert_array_equal(ex.to_host(sv), w, err_msg=f"config {cfg} {kdt}")
+    ex.sync()
