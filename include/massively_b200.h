@@ -413,6 +413,24 @@ int mb_tune_get(mb_executor* exec, int family);
 /* Human-readable description of one configuration (static string). */
 const char* mb_tune_describe(int family, int config);
 
+/* ------------------------------------------------------- kernel timing ---- */
+
+/* No counterpart in massively (which has no tracing).  While enabled, the
+ * executor brackets each launch of its dominant kernels with CUDA events on
+ * its stream (never inside a graph capture).  mb_kernel_timing_read
+ * synchronises the stream and returns, for one MB_KF_* family, how many
+ * launches were recorded since the last read of that family and their summed
+ * device time in milliseconds, then forgets them.  Used by the benchmark for
+ * the per-kernel roofline. */
+enum {
+  MB_KF_RADIX_ONESWEEP = 0,  /* one onesweep digit pass */
+  MB_KF_RADIX_HISTOGRAM = 1, /* the all-digit histogram */
+  MB_KF_SCAN = 2,            /* inclusive / exclusive scan */
+  MB_KF_SELECT = 3           /* copy_where / remove_where / partition */
+};
+int mb_kernel_timing(mb_executor* exec, int enable);
+int mb_kernel_timing_read(mb_executor* exec, int family, uint64_t* launches, double* total_ms);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -19,6 +19,7 @@ OK, LENGTH_MISMATCH, OUTPUT_TOO_SHORT, LENGTH_TOO_LARGE, INVALID_SEGMENTATION, \
     UNBOUND_COLUMN, FOREIGN_EXECUTOR, LAUNCH = range(8)
 SRC_COLUMN, SRC_CONSTANT, SRC_COUNTING, SRC_STRIDE, SRC_PERMUTE, SRC_REVERSE, \
     SRC_REPEAT_EACH, SRC_TILE, SRC_ADJACENT = range(9)
+KF_RADIX_ONESWEEP, KF_RADIX_HISTOGRAM, KF_SCAN, KF_SELECT = range(4)
 
 
 class mb_src(C.Structure):
@@ -107,6 +108,8 @@ def _declare(L: C.CDLL) -> None:
         "mb_tune_set": (i32, [vp, i32, i32]),
         "mb_tune_get": (i32, [vp, i32]),
         "mb_tune_describe": (C.c_char_p, [i32, i32]),
+        "mb_kernel_timing": (i32, [vp, i32]),
+        "mb_kernel_timing_read": (i32, [vp, i32, _P(u64), _P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name, None)

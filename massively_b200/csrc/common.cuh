@@ -10,6 +10,7 @@
 
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/massively_b200.h"
 
@@ -379,6 +380,13 @@ struct mb_executor {
   int tune[8];             // selected configuration per MB_TUNE_* family (-1 default)
   bool capturing;
   cudaGraph_t graph;
+  // mb_kernel_timing: event pairs around the dominant kernels' launches.
+  struct Span {
+    int family;
+    cudaEvent_t start, stop;
+  };
+  bool timing = false;
+  std::vector<Span> spans;
 };
 
 namespace mb {
@@ -396,6 +404,29 @@ int check_cuda(cudaError_t e, const char* what);
     int s_ = (call);                  \
     if (s_ != MB_OK) return s_;       \
   } while (0)
+
+// Brackets the launches issued in its scope with CUDA events on the
+// executor's stream while mb_kernel_timing is on (never inside a capture).
+struct TimedLaunch {
+  mb_executor* ex;
+  int family;
+  cudaEvent_t start = nullptr;
+  TimedLaunch(mb_executor* e, int fam) : ex(e), family(fam) {
+    if (!ex->timing || ex->capturing) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ex->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+      return;
+    if (cudaEventCreate(&start) != cudaSuccess) { start = nullptr; return; }
+    cudaEventRecord(start, ex->stream);
+  }
+  ~TimedLaunch() {
+    if (!start) return;
+    cudaEvent_t stop = nullptr;
+    if (cudaEventCreate(&stop) != cudaSuccess) { cudaEventDestroy(start); return; }
+    cudaEventRecord(stop, ex->stream);
+    ex->spans.push_back({family, start, stop});
+  }
+};
 
 // Stream-ordered scratch from the executor's pool, released at scope end
 // (in stream order, so it stays valid for every kernel enqueued before).

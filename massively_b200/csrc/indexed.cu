@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Src values, Src idx, S
             typename std::conditional<SIZE == 4, uint32_t, uint64_t>::type>::type>::type;
   uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x;
   const uint64_t step = (uint64_t)gridDim.x * kThreads;
-  for (; i < n; i += step) {
+  const uint64_t lim = src_len(idx) < n ? src_len(idx) : n;  // the indices' logical length
+  for (; i < lim; i += step) {
     if (has_stencil && src_load<uint32_t>(stencil, i) == 0) continue;
     const uint64_t j = src_load<uint32_t>(idx, i);
     if (j >= nvalues) { raise_device_error(status, MB_DEV_ERR_BOUNDS); continue; }
@@ -203,7 +204,7 @@ int launch_indexed(mb_executor* ex, const mb_src* values, const mb_src* indices,
 
 // Internal: dst[i] = src[idx[i]] for plain columns of `esize`-byte elements.
 int gather_raw(mb_executor* ex, const void* src, size_t esize, uint64_t nsrc,
-               const uint32_t* idx, uint64_t n, void* dst) {
+               const uint32_t* idx, uint64_t n, void* dst, const uint32_t* n_dev) {
   if (n == 0) return MB_OK;
   Src v{};
   v.kind = MB_SRC_COLUMN;
@@ -217,6 +218,7 @@ int gather_raw(mb_executor* ex, const void* src, size_t esize, uint64_t nsrc,
   ix.map = MB_UN_IDENTITY;
   ix.data = idx;
   ix.len = n;
+  ix.len_dev = n_dev;  // only the first *n_dev indices when given
   const unsigned g = stride_grid(n);
   switch (esize) {
     case 1: gather_kernel<1><<<g, kThreads, 0, ex->stream>>>(v, ix, Src{}, false, dst, n, nsrc, ex->status_dev); break;

@@ -52,22 +52,6 @@ __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
   return (uint32_t)((enc_bits<K, ENC>(k) >> shift) & (kBins - 1));
 }
 
-// Lanes holding the same 8-bit digit as this lane (digit kBins = no item:
-// matches the other empty lanes only), from one ballot per digit bit plus a
-// validity ballot -- cheaper than match.any under a full SM's load.
-__device__ __forceinline__ unsigned match_digit(uint32_t d) {
-  const bool valid = d < (uint32_t)kBins;
-  const unsigned vb = __ballot_sync(kFull, valid);
-  unsigned m = valid ? vb : ~vb;
-#pragma unroll
-  for (int b = 0; b < kRadixBits; ++b) {
-    const bool bit = (d >> b) & 1u;
-    const unsigned bal = __ballot_sync(kFull, bit);
-    m &= bit ? bal : ~bal;
-  }
-  return m;
-}
-
 // Buffer plan of one sort, filled on the device by the plan kernel.
 struct PassPlan {
   const void* in_k[8];
@@ -76,7 +60,8 @@ struct PassPlan {
   void* out_v[8];
   uint32_t active[8];
   uint32_t copy_only;
-  uint32_t pad_[3];
+  uint32_t n;  // items sorted: the capacity, or the device length when one is given
+  uint32_t pad_[2];
 };
 
 // ----------------------------------------------------------- histogram --
@@ -91,7 +76,9 @@ struct PassPlan {
 // the last full chunk, go one key per thread.
 template <class K, int ENC, int PASSES>
 __global__ void __launch_bounds__(kHistThreads, 2)
-    radix_histogram_kernel(const K* __restrict__ keys, uint64_t n, uint32_t* __restrict__ hist) {
+    radix_histogram_kernel(const K* __restrict__ keys, uint64_t n, const uint32_t* __restrict__ n_dev,
+                           uint32_t* __restrict__ hist) {
+  if (n_dev && *n_dev < n) n = *n_dev;
   constexpr int COPIES = 16 / PASSES;
   constexpr int KPV = 16 / (int)sizeof(K);      // keys per 16-byte vector
   constexpr int KPL = KPV * kHistUnroll;        // keys per lane per chunk
@@ -161,9 +148,11 @@ __global__ void __launch_bounds__(kHistThreads, 2)
 // One block of 256 threads: exclusive digit offsets per pass (in place over
 // `hist`), trivial-pass detection and the buffer assignment.
 __global__ void __launch_bounds__(kBins)
-    radix_plan_kernel(uint32_t* __restrict__ hist, int passes, uint64_t n, PassPlan* plan,
-                      const void* in_k, void* out_k, void* tmp_k, const void* in_v, void* out_v,
-                      void* tmp_v) {
+    radix_plan_kernel(uint32_t* __restrict__ hist, int passes, uint64_t n,
+                      const uint32_t* __restrict__ n_dev, PassPlan* plan, const void* in_k,
+                      void* out_k, void* tmp_k, const void* in_v, void* out_v, void* tmp_v) {
+  if (n_dev && *n_dev < n) n = *n_dev;
+  if (threadIdx.x == 0) plan->n = (uint32_t)n;
   __shared__ uint32_t s_scan[kBins];
   __shared__ uint32_t s_trivial[8];
   const int d = threadIdx.x;
@@ -242,6 +231,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
                           uint32_t* __restrict__ counter, DevErr err) {
   constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
   using S = OnesweepSmem<K, V, THREADS, ITEMS>;
+  if (plan->n < n) n = plan->n;  // device length
   constexpr int WARPS = S::WARPS;
   constexpr int TILE = S::TILE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -543,18 +533,17 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
   }
   __syncthreads();
   if (tid < kBins) {
-    uint32_t add = 0;
-    for (int w = 0; w < warp; ++w) add += sm.wsum[w];
-    sm.tile_start[tid] += add;
+    uint32_t start = sm.tile_start[tid];
+    for (int w = 0; w < warp; ++w) start += sm.wsum[w];
+    sm.tile_start[tid] = start;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) sm.warp_cnt[w][tid] += start;  // warp's first tile position
   }
   __syncthreads();
 
   // Keys to their tile-sorted positions (in place: all were read above).
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t d = rd[k] >> 16;
-    rd[k] = (rd[k] & 0xFFFFu) + sm.tile_start[d & (kBins - 1)] + sm.warp_cnt[warp][d];
-  }
+  for (int k = 0; k < ITEMS; ++k) rd[k] = (rd[k] & 0xFFFFu) + sm.warp_cnt[warp][rd[k] >> 16];
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k)
     if (FULL || wl + k * 32 < valid) sm.keys[rd[k]] = key[k];
@@ -635,6 +624,7 @@ __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THRE
   constexpr bool KEYS_ONLY = S::KEYS_ONLY;
   constexpr int WARPS = S::WARPS;
   constexpr int TILE = S::TILE;
+  if (plan->n < n) n = plan->n;  // device length
   extern __shared__ __align__(128) unsigned char smem_tma[];
   S& sm = *reinterpret_cast<S*>(smem_tma);
   const int tid = threadIdx.x;
@@ -710,7 +700,7 @@ constexpr int kRadixDefault32 = 2;  // 32-bit keys, values of at most 32 bits
 
 template <class K, int ENC, class V, int THREADS, int ITEMS, int NT = 1>
 int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v,
-                      uint64_t n) {
+                      uint64_t n, const uint32_t* n_dev) {
   constexpr int PASSES = (int)sizeof(K);
   constexpr int TILE = THREADS * ITEMS;
   constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
@@ -744,11 +734,14 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   // most two blocks per SM stay resident.
   const uint64_t hist_blocks = std::min<uint64_t>((n + kHistThreads * 16 - 1) / (kHistThreads * 16),
                                                   (uint64_t)sms * 2);
-  radix_histogram_kernel<K, ENC, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks), kHistThreads,
-                                      0, ex->stream>>>(in_k, n, hist);
+  {
+    TimedLaunch timed(ex, MB_KF_RADIX_HISTOGRAM);
+    radix_histogram_kernel<K, ENC, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks),
+                                             kHistThreads, 0, ex->stream>>>(in_k, n, n_dev, hist);
+  }
   MB_CUDA(cudaGetLastError());
-  radix_plan_kernel<<<1, kBins, 0, ex->stream>>>(hist, PASSES, n, plan, in_k, final_k, tmp_k,
-                                                 in_v, out_v, tmp_v);
+  radix_plan_kernel<<<1, kBins, 0, ex->stream>>>(hist, PASSES, n, n_dev, plan, in_k, final_k,
+                                                 tmp_k, in_v, out_v, tmp_v);
   MB_CUDA(cudaGetLastError());
   const DevErr err{ex->status_dev, counters + 32};
   const bool aligned = (uintptr_t)in_k % 16 == 0 && (uintptr_t)final_k % 16 == 0 &&
@@ -758,8 +751,11 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
     auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS, NT>;
     MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int p = 0; p < PASSES; ++p) {
-      kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
-          plan, p, (uint32_t)n, hist, status + (size_t)p * tiles * kBins, counters + p, err);
+      {
+        TimedLaunch timed(ex, MB_KF_RADIX_ONESWEEP);
+        kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
+            plan, p, (uint32_t)n, hist, status + (size_t)p * tiles * kBins, counters + p, err);
+      }
       MB_CUDA(cudaGetLastError());
     }
     return MB_OK;
@@ -768,25 +764,29 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   auto kern = radix_onesweep_kernel<K, ENC, V, THREADS, ITEMS>;
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int p = 0; p < PASSES; ++p) {
-    kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
-        plan, p, n, hist, status + (size_t)p * tiles * kBins, counters + p, err);
+    {
+      TimedLaunch timed(ex, MB_KF_RADIX_ONESWEEP);
+      kern<<<(unsigned)tiles, THREADS, smem, ex->stream>>>(
+          plan, p, n, hist, status + (size_t)p * tiles * kBins, counters + p, err);
+    }
     MB_CUDA(cudaGetLastError());
   }
   return MB_OK;
 }
 
 template <class K, int ENC, class V>
-int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v, uint64_t n) {
+int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v, uint64_t n,
+                  const uint32_t* n_dev) {
   if (n == 0) return MB_OK;
   int cfg = ex->tune[MB_TUNE_RADIX];
   if (cfg < 0) cfg = (sizeof(K) == 4 && sizeof(V) <= 4) ? kRadixDefault32 : kRadixDefault;
   switch (cfg) {
-    case 1: return onesweep_sort_cfg<K, ENC, V, 256, 16, 3>(ex, in_k, in_v, out_k, out_v, n);
-    case 2: return onesweep_sort_cfg<K, ENC, V, 512, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
-    case 3: return onesweep_sort_cfg<K, ENC, V, 256, 12, 3>(ex, in_k, in_v, out_k, out_v, n);
-    case 4: return onesweep_sort_cfg<K, ENC, V, 1024, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
-    case 5: return onesweep_sort_cfg<K, ENC, V, 384, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
-    default: return onesweep_sort_cfg<K, ENC, V, 256, 16, 1>(ex, in_k, in_v, out_k, out_v, n);
+    case 1: return onesweep_sort_cfg<K, ENC, V, 256, 16, 3>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 2: return onesweep_sort_cfg<K, ENC, V, 512, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 3: return onesweep_sort_cfg<K, ENC, V, 256, 12, 3>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 4: return onesweep_sort_cfg<K, ENC, V, 1024, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 5: return onesweep_sort_cfg<K, ENC, V, 384, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    default: return onesweep_sort_cfg<K, ENC, V, 256, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
   }
 }
 
@@ -794,13 +794,13 @@ int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* ou
 // integer type of the key's width, ENC its element type's encoding.
 template <class K, int ENC>
 int sort_keys_vals(mb_executor* ex, const void* ik, const void* iv, void* ok, void* ov,
-                   size_t vsize, uint64_t n) {
+                   size_t vsize, uint64_t n, const uint32_t* n_dev) {
   switch (vsize) {
-    case 0: return onesweep_sort<K, ENC, uint8_t>(ex, (const K*)ik, nullptr, (K*)ok, nullptr, n);
+    case 0: return onesweep_sort<K, ENC, uint8_t>(ex, (const K*)ik, nullptr, (K*)ok, nullptr, n, n_dev);
     case 4: return onesweep_sort<K, ENC, uint32_t>(ex, (const K*)ik, (const uint32_t*)iv, (K*)ok,
-                                                   (uint32_t*)ov, n);
+                                                   (uint32_t*)ov, n, n_dev);
     case 8: return onesweep_sort<K, ENC, uint64_t>(ex, (const K*)ik, (const uint64_t*)iv, (K*)ok,
-                                                   (uint64_t*)ov, n);
+                                                   (uint64_t*)ov, n, n_dev);
     default: return set_error(MB_ERR_LAUNCH, "radix values must be 4 or 8 bytes wide");
   }
 }
@@ -808,16 +808,18 @@ int sort_keys_vals(mb_executor* ex, const void* ik, const void* iv, void* ok, vo
 }  // namespace
 
 // Radix sort of plain device columns: keys of type `kdt` (32- or 64-bit
-// elements), values of `vsize` bytes (0 = none).  out_k may be null.
+// elements), values of `vsize` bytes (0 = none).  out_k may be null.  With
+// `n_dev`, only the first min(*n_dev, n) items are sorted (a count left on
+// the device by an earlier step; no host synchronisation).
 int radix_sort_plain(mb_executor* ex, int kdt, const void* ik, const void* iv, void* ok, void* ov,
-                     size_t vsize, uint64_t n) {
+                     size_t vsize, uint64_t n, const uint32_t* n_dev) {
   switch (kdt) {
-    case MB_U32: return sort_keys_vals<uint32_t, kEncUnsigned>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_I32: return sort_keys_vals<uint32_t, kEncSigned>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_F32: return sort_keys_vals<uint32_t, kEncFloat>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_U64: return sort_keys_vals<uint64_t, kEncUnsigned>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_I64: return sort_keys_vals<uint64_t, kEncSigned>(ex, ik, iv, ok, ov, vsize, n);
-    case MB_F64: return sort_keys_vals<uint64_t, kEncFloat>(ex, ik, iv, ok, ov, vsize, n);
+    case MB_U32: return sort_keys_vals<uint32_t, kEncUnsigned>(ex, ik, iv, ok, ov, vsize, n, n_dev);
+    case MB_I32: return sort_keys_vals<uint32_t, kEncSigned>(ex, ik, iv, ok, ov, vsize, n, n_dev);
+    case MB_F32: return sort_keys_vals<uint32_t, kEncFloat>(ex, ik, iv, ok, ov, vsize, n, n_dev);
+    case MB_U64: return sort_keys_vals<uint64_t, kEncUnsigned>(ex, ik, iv, ok, ov, vsize, n, n_dev);
+    case MB_I64: return sort_keys_vals<uint64_t, kEncSigned>(ex, ik, iv, ok, ov, vsize, n, n_dev);
+    case MB_F64: return sort_keys_vals<uint64_t, kEncFloat>(ex, ik, iv, ok, ov, vsize, n, n_dev);
     default: return set_error(MB_ERR_LAUNCH, "radix keys must be 32- or 64-bit elements");
   }
 }

@@ -155,6 +155,10 @@ int mb_executor_destroy(mb_executor* ex) {
   if (!ex) return MB_OK;
   cudaSetDevice(ex->device);
   cudaStreamSynchronize(ex->stream);
+  for (auto& sp : ex->spans) {
+    cudaEventDestroy(sp.start);
+    cudaEventDestroy(sp.stop);
+  }
   if (ex->graph) cudaGraphDestroy(ex->graph);
   cudaFree(ex->status_dev);
   cudaFreeHost(ex->host_pinned);
@@ -283,3 +287,37 @@ int mb_graph_destroy(mb_graph* g) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------- kernel timing --
+
+int mb_kernel_timing(mb_executor* ex, int enable) {
+  if (!ex) return mb::set_error(MB_ERR_LAUNCH, "null executor");
+  ex->timing = enable != 0;
+  return MB_OK;
+}
+
+int mb_kernel_timing_read(mb_executor* ex, int family, uint64_t* launches, double* total_ms) {
+  if (!ex) return mb::set_error(MB_ERR_LAUNCH, "null executor");
+  MB_CUDA(cudaSetDevice(ex->device));
+  MB_CUDA(cudaStreamSynchronize(ex->stream));
+  uint64_t count = 0;
+  double ms = 0.0;
+  std::vector<mb_executor::Span> keep;
+  for (auto& sp : ex->spans) {
+    if (sp.family != family) {
+      keep.push_back(sp);
+      continue;
+    }
+    float t = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&t, sp.start, sp.stop);
+    cudaEventDestroy(sp.start);
+    cudaEventDestroy(sp.stop);
+    if (e != cudaSuccess) continue;
+    ms += t;
+    ++count;
+  }
+  ex->spans.swap(keep);
+  if (launches) *launches = count;
+  if (total_ms) *total_ms = ms;
+  return MB_OK;
+}

@@ -419,6 +419,7 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
       scan_kernel<T, OPID, false, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
     }                                                                                           \
   } while (0)
+  TimedLaunch timed(ex, MB_KF_SCAN);
   switch (op) {
     case MB_OP_ADD: MB_SCAN_LAUNCH(MB_OP_ADD); break;
     case MB_OP_MIN: MB_SCAN_LAUNCH(MB_OP_MIN); break;

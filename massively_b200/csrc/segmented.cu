@@ -751,7 +751,11 @@ int mb_reduce_by_key_segmented(mb_executor* ex, const mb_src* keys, int key_eq,
     MB_CUDA(cudaMemsetAsync(count_dev, 0, 4, ex->stream));
   } else {
     for (int c = 0; c < nvals; ++c) {
-      MB_TRY(seg_entry(ex, &values[c], ops[c], kReduce, &inits[c], out_values[c].data,
+      // The keys' device length (a count left by an earlier step) bounds
+      // value views that carry none, such as a constant column.
+      mb_src v = values[c];
+      if (!v.len_dev) v.len_dev = keys->len_dev;
+      MB_TRY(seg_entry(ex, &v, ops[c], kReduce, &inits[c], out_values[c].data,
                        out_values[c].dtype, offsets, segment_count, keys,
                        c == 0 ? out_keys.data : nullptr,
                        (int)dtype_size(out_keys.dtype), c == 0 ? count_dev : nullptr));

@@ -305,6 +305,7 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
     auto st = TileState<uint32_t, true>::make(scratch.as<char>() + 256, tiles);
     const bool aligned = (uintptr_t)in[0].data % 16 == 0 &&
                          (p.fused || (uintptr_t)stencil->data % 16 == 0);
+    TimedLaunch timed(ex, MB_KF_SELECT);
     if (fast && aligned && mode != kPartition) {
       const int cols = p.fused ? 1 : 2;
       const size_t smem = (size_t)cols * kSmemTile * 4;

@@ -31,9 +31,9 @@
 namespace mb {
 
 int radix_sort_plain(mb_executor* ex, int kdt, const void* ik, const void* iv, void* ok, void* ov,
-                     size_t vsize, uint64_t n);
+                     size_t vsize, uint64_t n, const uint32_t* n_dev = nullptr);
 int gather_raw(mb_executor* ex, const void* src, size_t esize, uint64_t nsrc,
-               const uint32_t* idx, uint64_t n, void* dst);
+               const uint32_t* idx, uint64_t n, void* dst, const uint32_t* n_dev = nullptr);
 int materialize(mb_executor* ex, const mb_src& in, void* dst);
 
 namespace {
@@ -56,7 +56,8 @@ template <class U, int ENC>
 __global__ void __launch_bounds__(kThreads)
     encode_keys_kernel(Src in, U* out, uint64_t n, int ieee, int desc) {
   constexpr U sign = (U)1 << (sizeof(U) * 8 - 1);
-  for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n;
+  const uint64_t lim = src_len(in) < n ? src_len(in) : n;  // the view's logical length
+  for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < lim;
        i += (uint64_t)gridDim.x * kThreads) {
     U raw = (U)src_load_bits(in, i);
     if (in.vtype == MB_I8) raw = (U)(uint32_t)(int32_t)(int8_t)raw;
@@ -75,9 +76,10 @@ __global__ void __launch_bounds__(kThreads) iota_kernel(uint32_t* out, uint64_t 
     out[i] = (uint32_t)i;
 }
 
+// A column read as stored (no view, no map, no cast); it may carry a device
+// length, which the sort honours.
 bool is_plain_column(const mb_src& s) {
-  return s.kind == MB_SRC_COLUMN && s.map == MB_UN_IDENTITY && s.dtype == s.vtype &&
-         s.len_dev == nullptr;
+  return s.kind == MB_SRC_COLUMN && s.map == MB_UN_IDENTITY && s.dtype == s.vtype;
 }
 bool wide_key_type(int dt) {
   return dt == MB_U32 || dt == MB_I32 || dt == MB_F32 || dt == MB_U64 || dt == MB_I64 ||
@@ -107,7 +109,7 @@ int encode_keys(mb_executor* ex, const Src& s, int vtype, void* out, uint64_t n,
 // The permutation path.  `modes[c]` / `descs[c]` per key column.
 int permutation_sort(mb_executor* ex, const mb_src* keys, int nk, const int* ieee,
                      const int* desc, const mb_src* values, int nv, const mb_col* out_values,
-                     const mb_col* out_keys, uint64_t n) {
+                     const mb_col* out_keys, uint64_t n, const uint32_t* n_dev) {
   Scratch perm_a, perm_b, ukeys, mat;
   MB_TRY(perm_a.alloc(ex, n * 4));
   MB_TRY(perm_b.alloc(ex, n * 4));
@@ -135,9 +137,10 @@ int permutation_sort(mb_executor* ex, const mb_src* keys, int nk, const int* iee
     s.data = col;
     s.index = cur;
     s.len = n;
+    s.len_dev = n_dev;
     MB_TRY(encode_keys(ex, s, keys[c].vtype, ukeys.ptr, n, ieee[c], desc[c]));
     const int udt = dtype_size(compute_type(keys[c].vtype)) == 8 ? MB_U64 : MB_U32;
-    MB_TRY(radix_sort_plain(ex, udt, ukeys.ptr, cur, nullptr, nxt, 4, n));
+    MB_TRY(radix_sort_plain(ex, udt, ukeys.ptr, cur, nullptr, nxt, 4, n, n_dev));
     std::swap(cur, nxt);
   }
   // Gather the outputs through the final permutation.
@@ -154,7 +157,7 @@ int permutation_sort(mb_executor* ex, const mb_src* keys, int nk, const int* iee
         MB_TRY(materialize(ex, s, tmp.ptr));
         col = tmp.ptr;
       }
-      MB_TRY(gather_raw(ex, col, dtype_size(s.vtype), n, cur, n, outs[c].data));
+      MB_TRY(gather_raw(ex, col, dtype_size(s.vtype), n, cur, n, outs[c].data, n_dev));
     }
   }
   return MB_OK;
@@ -207,13 +210,18 @@ int sort_general(mb_executor* ex, const mb_src* keys, int nk, const int* ieee, c
                       (nv == 0 || (nv == 1 && is_plain_column(values[0]) &&
                                    (dtype_size(values[0].vtype) == 4 ||
                                     dtype_size(values[0].vtype) == 8)));
+  // A device length (a count left on the device by copy_where and the like)
+  // bounds every kernel on the device; the host sizes by capacity.
+  const uint32_t* n_dev = nullptr;
+  for (int c = 0; c < nk && !n_dev; ++c) n_dev = keys[c].len_dev;
+  for (int c = 0; c < nv && !n_dev; ++c) n_dev = values[c].len_dev;
   if (direct) {
     const size_t vs = nv ? dtype_size(values[0].vtype) : 0;
     return radix_sort_plain(ex, keys[0].vtype, keys[0].data, nv ? values[0].data : nullptr,
                             out_keys ? out_keys[0].data : nullptr,
-                            nv ? out_values[0].data : nullptr, vs, n);
+                            nv ? out_values[0].data : nullptr, vs, n, n_dev);
   }
-  return permutation_sort(ex, keys, nk, ieee, desc, values, nv, out_values, out_keys, n);
+  return permutation_sort(ex, keys, nk, ieee, desc, values, nv, out_values, out_keys, n, n_dev);
 }
 
 void comparator_mode(int less, int vtype, int* ieee, int* desc) {

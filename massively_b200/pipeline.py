@@ -1,0 +1,67 @@
+"""Multi-step pipelines over device counts, and their capture as CUDA graphs.
+
+`group_by` is the filter -> sort -> aggregate -> join chain of the group-by
+configuration: rows whose flag is set are kept (copy_where, count left on the
+device), sorted by key (the sort reads that count on the device), reduced per
+key run into (sum, count, min) (reduce_by_key with a constant-one column), and
+the distinct keys are intersected with a sorted list (set_intersection).  No
+step reads a count back to the host, so the whole chain can be captured once
+and replayed: `Captured` records it into a CUDA graph (torch's graph capture,
+with the executor bound to the capturing stream; the library's stream-ordered
+scratch becomes graph allocations) and `replay` relaunches every kernel with
+one call.  Inputs are read from the buffers given at capture time, so new
+data is copied into those buffers before a replay.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import lazy, vector
+from . import op as O
+from .iter import Zip
+from .runtime import DeviceVec, Executor
+
+
+def group_by(exec: Executor, keys: DeviceVec, values: DeviceVec, flag: DeviceVec,
+             other: DeviceVec) -> dict:
+    """keys u32, values f32, flag u32 (non-zero = keep), other sorted u32.
+    Returns device vectors (each with its count on the device): the distinct
+    kept keys in order, per key the f32 sum, u32 count and f32 min of its
+    values, and the distinct keys also present in `other`."""
+    kept = vector.copy_where(exec, Zip(keys, values), flag)
+    k1, v1 = kept.cols
+    sk, sv = vector.radix_sort_pairs(exec, k1, v1)
+    ones = lazy.constant(1, np.uint32).take(len(sk))
+    rk, agg = vector.reduce_by_key(exec, sk, Zip(sv, ones, sv), O.Equal,
+                                   (np.float32(0), np.uint32(0), np.float32(np.inf)),
+                                   (O.Add, O.Add, O.Min))
+    s, c, m = agg.cols
+    common = vector.set_intersection(exec, rk, other)
+    return {"keys": rk, "sum": s, "count": c, "min": m, "common": common,
+            "kept": k1}
+
+
+class Captured:
+    """`fn(exec)` captured once into a CUDA graph; `replay()` relaunches it on
+    the current stream.  The outputs `fn` returned are kept (their buffers
+    are rewritten by each replay)."""
+
+    def __init__(self, exec: Executor, fn, warmup: int = 1):
+        self.exec = exec
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            exec.bind_current_stream()
+            for _ in range(warmup):  # loads kernels and fills the pools outside capture
+                fn(exec)
+        torch.cuda.current_stream().wait_stream(side)
+        exec.sync()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            exec.bind_current_stream()
+            self.outputs = fn(exec)
+        exec.bind_current_stream()
+
+    def replay(self) -> None:
+        self.graph.replay()

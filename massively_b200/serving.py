@@ -1,23 +1,23 @@
 """Continuous-batching request loop over the primitive kernels.
 
 Requests (sort_by_key u32/u32, inclusive_scan u32, reduce_by_key u32/f32)
-arrive on a Poisson clock with sizes log-uniform on [2^10, 2^26].  The loop
-admits arrived requests while their device buffers fit in a memory budget,
-coalesces the small admitted requests of one kind into one segmented launch
-(segment ids as the leading sort key, `seg` scans, or (segment, key)
-run keys for reduce_by_key -- runs never cross request boundaries), runs
-large requests on their own, keeps up to `streams` launches in flight on
-separate CUDA streams, and retires requests when their completion event
-fires.  Latency is completion time (from CUDA events on a common reference)
-minus arrival time.  `plain_dispatch` serves the same trace one request per
-launch in arrival order, for comparison.
+arrive on a Poisson clock with sizes log-uniform on [2^10, 2^26] and wait in
+a queue.  Whenever one of the loop's stream slots frees up, the head of the
+queue is launched: alone if it is large, else together with every waiting
+small request of its kind as one segmented launch (segment ids as the
+leading sort key; `seg` inclusive scans; reduce_by_key whose runs also break
+at request boundaries), so requests that arrive while the GPU is busy
+accumulate into larger batches.  Launches are admitted while the device
+bytes of everything in flight fit a memory budget, run on several CUDA
+streams so their work overlaps, and retire when their completion events
+fire.  Latency is completion time (CUDA events on a common reference) minus
+arrival time.  `plain_dispatch` serves the same trace one request per launch
+in arrival order, for comparison.
 
-Results are the same alone and in the mix: integer outputs bit-exact, f32
-sums within the association bound (tests/test_serving_gpu.py).
+Results are the same alone and in the mix (tests/test_serving_gpu.py).
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
 import time
 from dataclasses import dataclass, field
@@ -28,7 +28,7 @@ import torch
 from . import _native as N
 from . import lazy
 from . import op as O
-from .runtime import DeviceVec, Executor, check
+from .runtime import Executor, check
 
 SORT, SCAN, RBK = "sort_by_key", "inclusive_scan", "reduce_by_key"
 
@@ -68,29 +68,44 @@ def make_trace(rate: float = 20_000.0, duration: float = 1.0, lo_log2: int = 10,
     return reqs
 
 
-def materialize_inputs(exec: Executor, r: Request) -> None:
-    """Device inputs of a request, from the PCG streams (no host copy)."""
+INPUTS = {SORT: (("keys", np.uint32), ("values", np.uint32)),
+          SCAN: (("x", np.uint32),),
+          RBK: (("keys", np.uint32), ("values", np.float32))}
+
+
+def materialize_inputs(exec: Executor, r: Request, into: dict | None = None) -> None:
+    """Device inputs of a request, from the PCG streams (no host copy),
+    written into `into` (columns of r.n items, e.g. slices of a batch's
+    buffers) or into fresh buffers."""
     from .vector import copy
+    cols = into or {name: exec.alloc(dt, r.n) for name, dt in INPUTS[r.kind]}
     if r.kind == SORT:
-        k = exec.alloc(np.uint32, r.n)
-        check(N.lib().mb_random_uniform_u32(exec.handle, 0, 0xFFFFFFFF, r.seed, 0, k.to_col()))
-        v = exec.alloc(np.uint32, r.n)
-        copy(exec, lazy.counting(0).take(r.n), v)
-        r.inputs = {"keys": k, "values": v}
+        check(N.lib().mb_random_uniform_u32(exec.handle, 0, 0xFFFFFFFF, r.seed, 0,
+                                            cols["keys"].to_col()))
+        copy(exec, lazy.counting(0).take(r.n), cols["values"])
     elif r.kind == SCAN:
-        x = exec.alloc(np.uint32, r.n)
-        check(N.lib().mb_random_uniform_u32(exec.handle, 0, 1000, r.seed, 0, x.to_col()))
-        r.inputs = {"x": x}
+        check(N.lib().mb_random_uniform_u32(exec.handle, 0, 1000, r.seed, 0, cols["x"].to_col()))
     else:
-        # sorted keys in runs of 8 (the group-by shape after sort_by_key)
-        kk = exec.alloc(np.uint32, r.n)
+        # sorted keys in runs of 8 (the group-by shape after sort_by_key);
+        # values are integers below 2^20 held as f32
         copy(exec, lazy.RepeatEach(lazy.counting(r.seed & 0xFFFF).take((r.n + 7) // 8), r.n,
-                                   a=8), kk)
+                                   a=8), cols["keys"])
         v = exec.alloc(np.uint32, r.n)
         check(N.lib().mb_random_uniform_u32(exec.handle, 0, 1 << 20, r.seed, 0, v.to_col()))
-        vf = exec.alloc(np.float32, r.n)
-        copy(exec, lazy.cast(v, np.float32), vf)
-        r.inputs = {"keys": kk, "values": vf}
+        copy(exec, lazy.cast(v, np.float32), cols["values"])
+    r.inputs = cols
+
+
+def materialize_batch(exec: Executor, reqs: list[Request]) -> dict:
+    """Inputs of a coalesced group, each request's written straight into its
+    slice of the batch's columns."""
+    total = sum(r.n for r in reqs)
+    batch = {name: exec.alloc(dt, total) for name, dt in INPUTS[reqs[0].kind]}
+    off = 0
+    for r in reqs:
+        materialize_inputs(exec, r, {k: v.slice(off, off + r.n) for k, v in batch.items()})
+        off += r.n
+    return batch
 
 
 # ------------------------------------------------------------ executors ----
@@ -109,36 +124,26 @@ def run_single(exec: Executor, r: Request) -> None:
         r.outputs = {"keys": k, "values": v}
 
 
-def _concat(exec, cols):
-    total = sum(len(c) for c in cols)
-    out = exec.alloc(cols[0].dtype, total)
-    off = 0
-    for c in cols:
-        out.tensor[off:off + len(c)].copy_(c.tensor)
-        off += len(c)
-    return out
-
-
 def _offsets(exec, reqs):
     off = np.zeros(len(reqs) + 1, np.uint32)
     off[1:] = np.cumsum([r.n for r in reqs])
     return exec.to_device(off), off
 
 
-def run_coalesced(exec: Executor, reqs: list[Request]) -> None:
-    """Several small requests of one kind in one segmented launch."""
+def run_coalesced(exec: Executor, reqs: list[Request], batch: dict) -> None:
+    """Several small requests of one kind, whose inputs sit back to back in
+    `batch` (materialize_batch), in one segmented launch."""
     from . import seg, vector
     kind = reqs[0].kind
     dev_off, host_off = _offsets(exec, reqs)
     sgm = seg.Segmentation(dev_off, int(host_off[-1]))
     if kind == SCAN:
-        x = _concat(exec, [r.inputs["x"] for r in reqs])
+        x = batch["x"]
         y = seg.ForEachSegment(seg.InclusiveScan(O.Add)).run(exec, sgm.segments(x)).values()
         for i, r in enumerate(reqs):
             r.outputs = {"y": y.slice(int(host_off[i]), int(host_off[i + 1]))}
     elif kind == SORT:
-        keys = _concat(exec, [r.inputs["keys"] for r in reqs])
-        vals = _concat(exec, [r.inputs["values"] for r in reqs])
+        keys, vals = batch["keys"], batch["values"]
         ids = sgm.segment_ids(exec)
         from .iter import Zip
         out = vector.radix_sort_by_key(exec, Zip(ids, keys), Zip(keys, vals))
@@ -147,8 +152,7 @@ def run_coalesced(exec: Executor, reqs: list[Request]) -> None:
             a, b = int(host_off[i]), int(host_off[i + 1])
             r.outputs = {"keys": sk.slice(a, b), "values": sv.slice(a, b)}
     else:
-        keys = _concat(exec, [r.inputs["keys"] for r in reqs])
-        vals = _concat(exec, [r.inputs["values"] for r in reqs])
+        keys, vals = batch["keys"], batch["values"]
         # runs break at request boundaries as well as at key changes
         k, v = vector.reduce_by_key_segmented(exec, keys, vals, O.Equal, np.float32(0), O.Add,
                                               dev_off)
@@ -199,22 +203,23 @@ class _Clock:
 
 
 def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
-          small_n: int = 1 << 20, max_batch: int = 256, streams: int = 4,
+          small_n: int = 1 << 20, max_batch: int = 256, streams: int = 4, depth: int = 2,
           keep_outputs: bool = False) -> ServeStats:
-    """Continuous batching: admit by memory, coalesce small requests, keep
-    `streams` launches in flight, retire on completion events."""
+    """Continuous batching.  Arrived requests wait in a queue; whenever one
+    of the `streams` launch slots (each holds up to `depth` launches in
+    flight) frees up, the head of the queue is launched: alone if it is
+    large, else together with every waiting small request of its kind (up to
+    `max_batch`) as one segmented launch.  Requests that arrive while the
+    GPU is busy therefore accumulate into larger batches.  A launch is
+    admitted only while the bytes of everything in flight stay within
+    `budget_bytes`; requests retire when their completion event fires."""
     pool = [torch.cuda.Stream() for _ in range(streams)]
     clock = _Clock()
-    pending = list(reqs)        # in arrival order
+    waiting: list[Request] = []
     inflight = []               # (event, [requests], bytes, stream index)
-    used = 0
-    max_used = 0
-    launches = 0
-    nxt = 0
-    done_count = 0
-    busy = [False] * streams
+    load = [0] * streams        # launches in flight per stream
+    used = max_used = launches = nxt = done_count = 0
     while done_count < len(reqs):
-        # retire finished launches
         still = []
         for ev, group, b, si in inflight:
             if ev.query():
@@ -226,68 +231,80 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
                     r.inputs = {}
                 used -= b
                 done_count += len(group)
-                busy[si] = False
+                load[si] -= 1
             else:
                 still.append((ev, group, b, si))
         inflight = still
-        # admit arrived requests while memory allows
         now = clock.now()
-        admitted = []
-        while nxt < len(pending) and pending[nxt].arrival <= now:
-            r = pending[nxt]
-            if used + r.bytes_needed() > budget_bytes and (inflight or admitted):
-                break
-            admitted.append(r)
-            used += r.bytes_needed()
+        while nxt < len(reqs) and reqs[nxt].arrival <= now:
+            waiting.append(reqs[nxt])
             nxt += 1
-        max_used = max(max_used, used)
-        if not admitted:
-            if not inflight and nxt < len(pending):
-                time.sleep(max(0.0, min(1e-3, pending[nxt].arrival - clock.now())))
-            continue
-        # group: small requests of a kind coalesce, large ones go alone
-        groups = []
-        for kind in (SORT, SCAN, RBK):
-            small = [r for r in admitted if r.kind == kind and r.n <= small_n]
-            for i in range(0, len(small), max_batch):
-                groups.append(small[i:i + max_batch])
-            groups += [[r] for r in admitted if r.kind == kind and r.n > small_n]
-        for group in groups:
-            si = next((i for i in range(streams) if not busy[i]), None)
-            if si is None:  # all streams busy: queue behind the least-loaded one
-                si = launches % streams
-            busy[si] = True
+        launched = False
+        while waiting:
+            si = min(range(streams), key=lambda i: load[i])
+            if load[si] >= depth:
+                break
+            head = waiting[0]
+            if head.n > small_n:
+                group = [head]
+            else:
+                group, room = [], budget_bytes - used
+                for r in waiting:
+                    if r.kind == head.kind and r.n <= small_n and len(group) < max_batch:
+                        if r.bytes_needed() > room and group:
+                            break
+                        group.append(r)
+                        room -= r.bytes_needed()
+            b = sum(r.bytes_needed() for r in group)
+            if used + b > budget_bytes and inflight:
+                break               # wait for memory to come back
+            ids = {id(r) for r in group}
+            waiting = [r for r in waiting if id(r) not in ids]
             with torch.cuda.stream(pool[si]):
                 exec.bind_current_stream()
-                for r in group:
-                    materialize_inputs(exec, r)
                 if len(group) == 1:
+                    materialize_inputs(exec, group[0])
                     run_single(exec, group[0])
                 else:
-                    run_coalesced(exec, group)
+                    run_coalesced(exec, group, materialize_batch(exec, group))
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record()
+            used += b
+            max_used = max(max_used, used)
+            load[si] += 1
             launches += 1
-            inflight.append((ev, group, sum(r.bytes_needed() for r in group), si))
+            launched = True
+            inflight.append((ev, group, b, si))
+        if not launched:
+            if not inflight and not waiting and nxt < len(reqs):
+                time.sleep(max(0.0, min(1e-3, reqs[nxt].arrival - clock.now())))
+            elif inflight:
+                time.sleep(20e-6)
     exec.bind_current_stream()
     torch.cuda.synchronize()
     t_end = max(r.done for r in reqs)
     return _stats(reqs, t_end, launches, max_used)
 
 
-def plain_dispatch(exec: Executor, reqs: list[Request], keep_outputs: bool = False) -> ServeStats:
-    """One request per launch, in arrival order, on one stream."""
+def plain_dispatch(exec: Executor, reqs: list[Request], keep_outputs: bool = False,
+                   wait: bool = True) -> ServeStats:
+    """One request per launch, in arrival order, on one stream.  With `wait`
+    (plain request/response serving) each request's result is waited for
+    before the next request is dispatched; without it the requests are
+    queued back to back on the stream, with no coalescing or overlap."""
     clock = _Clock()
     events = []
     for r in reqs:
-        wait = r.arrival - clock.now()
-        if wait > 0:
-            time.sleep(wait)
+        delay = r.arrival - clock.now()
+        if delay > 0:
+            time.sleep(delay)
         materialize_inputs(exec, r)
         run_single(exec, r)
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
         events.append(ev)
+        if wait:
+            ev.synchronize()
         if not keep_outputs:
             # stream-ordered frees: the memory is reused only by later work
             # on this stream

@@ -81,6 +81,15 @@ def _len_dev_of(x):
     return c.len_dev if isinstance(c, DeviceVec) else None
 
 
+def _first_len_dev(*xs):
+    # (never truth-test a device tensor: that reads it back, a sync)
+    for x in xs:
+        ld = _len_dev_of(x)
+        if ld is not None:
+            return ld
+    return None
+
+
 def _count_buffer(exec: Executor) -> torch.Tensor:
     return torch.zeros(1, dtype=torch.uint32, device=f"cuda:{exec.device}")
 
@@ -322,7 +331,7 @@ def radix_sort_by_key(exec: Executor, keys, values):
     keep = []
     ks, nk = _srcs(exec, keys, keep)
     vs, nv = _srcs(exec, values, keep)
-    outs = _out_like(exec, values, n)
+    outs = _out_like(exec, values, n, _first_len_dev(keys, values))
     check(_L().mb_radix_sort_by_key(exec.handle, ks, nk, vs, nv, _cols(outs), None))
     return _wrap(values, outs)
 
@@ -336,8 +345,9 @@ def radix_sort_pairs(exec: Executor, keys, values):
     keep = []
     ks, nk = _srcs(exec, keys, keep)
     vs, nv = _srcs(exec, values, keep)
-    kout = _out_like(exec, keys, n)
-    vout = _out_like(exec, values, n)
+    ld = _first_len_dev(keys, values)  # a device count carries over
+    kout = _out_like(exec, keys, n, ld)
+    vout = _out_like(exec, values, n, ld)
     check(_L().mb_radix_sort_by_key(exec.handle, ks, nk, vs, nv, _cols(vout), _cols(kout)))
     return _wrap(keys, kout), _wrap(values, vout)
 

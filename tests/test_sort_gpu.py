@@ -184,3 +184,31 @@ def test_every_radix_config_bit_exact(n, keyspace):
             w = want if kdt == np.uint32 else orc.radix_perm([k])
             np.testing.assert_array_equal(ex.to_host(sv), w, err_msg=f"config {cfg} {kdt}")
     ex.sync()
+
+
+def test_kernel_timing_counts_onesweep_launches():
+    """mb_kernel_timing brackets each onesweep pass and the histogram."""
+    import ctypes as C
+    from massively_b200 import _native as N, vector
+    ex = executor()
+    L = N.lib()
+    n = 1 << 20
+    keys, vals = ex.to_device(seeded(np.uint32, n, 9)), ex.to_device(_perm_values(n))
+    for fam in range(4):
+        L.mb_kernel_timing_read(ex.handle, fam, None, None)
+    L.mb_kernel_timing(ex.handle, 1)
+    vector.radix_sort_pairs(ex, keys, vals)
+    vector.radix_sort_pairs(ex, keys, vals)
+    L.mb_kernel_timing(ex.handle, 0)
+    vector.radix_sort_pairs(ex, keys, vals)  # not recorded
+    got = {}
+    for fam in (N.KF_RADIX_ONESWEEP, N.KF_RADIX_HISTOGRAM, N.KF_SCAN):
+        cnt, ms = C.c_uint64(), C.c_double()
+        assert L.mb_kernel_timing_read(ex.handle, fam, C.byref(cnt), C.byref(ms)) == 0
+        got[fam] = (cnt.value, ms.value)
+    assert got[N.KF_RADIX_ONESWEEP][0] == 8 and got[N.KF_RADIX_ONESWEEP][1] > 0
+    assert got[N.KF_RADIX_HISTOGRAM][0] == 2
+    assert got[N.KF_SCAN] == (0, 0.0)
+    cnt = C.c_uint64()
+    L.mb_kernel_timing_read(ex.handle, N.KF_RADIX_ONESWEEP, C.byref(cnt), None)
+    assert cnt.value == 0  # read forgets
