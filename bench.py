@@ -695,7 +695,11 @@ def run_ours(args):
     step_achieved = wl.alg_bytes() / (ms * 1e-3) / 1e9
     # the dominant kernel alone: its algorithmic bytes over its own launches'
     # event-timed duration inside the timed region
-    achieved = wl.family_bytes() * args.steps / (kt["ms"] * 1e-3) / 1e9
+    if wl.family is not None:
+        achieved = wl.family_bytes() * args.steps / (kt["ms"] * 1e-3) / 1e9
+    else:  # a multi-kernel step (segmented, group-by): its byte model over the step time
+        achieved = step_achieved
+        kt = {"launches": 0, "ms": 0.0}
     secondary = {}
     if not args.no_secondary and args.workload == "sort_pairs_u32":
         del wl.keys, wl.vals, wl.ko, wl.vo
@@ -743,8 +747,9 @@ def run_ours(args):
                          "traffic": NCU_TRAFFIC_BYTES.get(wl.name),
                          "kernel": wl.kernel, "kernel_launches": kt["launches"],
                          "kernel_ms_per_launch": kt["ms"] / max(1, kt["launches"]),
-                         "alg_bytes_per_launch": wl.family_bytes() * args.steps
-                                                 / max(1, kt["launches"]),
+                         "alg_bytes_per_launch": (wl.family_bytes() * args.steps
+                                                  / max(1, kt["launches"]))
+                                                 if wl.family is not None else None,
                          "step_achieved": step_achieved, "step_frac": step_achieved / peak,
                          "note": "achieved = the dominant kernel's algorithmic bytes / its "
                                  "CUDA-event time over the timed region; step_* = the whole "

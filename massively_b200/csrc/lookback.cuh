@@ -120,17 +120,80 @@ __device__ __forceinline__ T ld_relaxed_any(const T* src) {
   return v;
 }
 
-// Status storage of one launch.  `words` (packed) or `flags`/`agg`/`incl`.
+// How a value shares one 64-bit status word with its 2-bit flag (the packed
+// layout).  4-byte values take the low word and the flag the high word;
+// other types may specialise this (the segmented kernels pack a 30-bit head
+// count beside a 4-byte value).
+template <class T>
+struct StatePack {
+  static constexpr bool kPackable = sizeof(T) == 4;
+  __device__ __forceinline__ static uint64_t pack(uint32_t flag, const T& v) {
+    return ((uint64_t)flag << 32) | to_bits64(v);
+  }
+  __device__ __forceinline__ static uint32_t unpack(uint64_t w, T& v) {
+    v = from_bits64<T>(w & 0xFFFFFFFFull);
+    return (uint32_t)(w >> 32);
+  }
+};
+
+// One value per slot, each with a "set" flag: the per-group states of the
+// grouped deterministic look-back.  Same two layouts as the tile states.
+template <class T, bool PACKED>
+struct Slots {
+  uint64_t* words;
+  uint32_t* flags;
+  T* vals;
+
+  static size_t bytes(uint64_t n) { return PACKED ? n * 8 : ((n * sizeof(T) + 63) / 64) * 64 + n * 4; }
+  static Slots make(void* base, uint64_t n) {
+    Slots s{};
+    if constexpr (PACKED) {
+      s.words = (uint64_t*)base;
+    } else {
+      s.vals = (T*)base;
+      s.flags = (uint32_t*)((char*)base + ((n * sizeof(T) + 63) / 64) * 64);
+    }
+    return s;
+  }
+  __device__ __forceinline__ void publish(uint64_t i, const T& v) const {
+    if constexpr (PACKED) {
+      st_relaxed_u64(words + i, StatePack<T>::pack(kFlagIncl, v));
+    } else {
+      st_relaxed_any(vals + i, v);
+      st_release_u32(flags + i, 1u);
+    }
+  }
+  __device__ __forceinline__ bool peek(uint64_t i, T& v) const {
+    if constexpr (PACKED) {
+      return StatePack<T>::unpack(ld_relaxed_u64(words + i), v) != kFlagNone;
+    } else {
+      if (ld_acquire_u32(flags + i) == 0) return false;
+      v = ld_relaxed_any(vals + i);
+      return true;
+    }
+  }
+};
+
+// Status storage of one launch.  `words` (packed) or `flags`/`agg`/`incl`,
+// plus the group states of the deterministic look-back (groups of 32
+// tiles: each group's aggregate and its inclusive prefix).
 template <class T, bool PACKED>
 struct TileState {
   uint64_t* words;
   uint32_t* flags;
   T* agg;
   T* incl;
+  Slots<T, PACKED> gagg, gincl;
 
-  static size_t bytes(uint64_t tiles) {
-    return PACKED ? tiles * 8 : tiles * (4 + 2 * sizeof(T)) + 64;
+  static uint64_t groups(uint64_t tiles) { return tiles / 32 + 1; }
+  static size_t main_bytes(uint64_t tiles) {
+    const size_t b = PACKED ? tiles * 8 : tiles * (4 + 2 * sizeof(T)) + 64;
+    return (b + 255) / 256 * 256;
   }
+  static size_t slots_bytes(uint64_t tiles) {
+    return (Slots<T, PACKED>::bytes(groups(tiles)) + 255) / 256 * 256;
+  }
+  static size_t bytes(uint64_t tiles) { return main_bytes(tiles) + 2 * slots_bytes(tiles); }
   static TileState make(void* base, uint64_t tiles) {
     TileState s{};
     if constexpr (PACKED) {
@@ -141,12 +204,15 @@ struct TileState {
       s.incl = (T*)(p + tiles * sizeof(T));
       s.flags = (uint32_t*)(p + 2 * tiles * sizeof(T));
     }
+    char* g = (char*)base + main_bytes(tiles);
+    s.gagg = Slots<T, PACKED>::make(g, groups(tiles));
+    s.gincl = Slots<T, PACKED>::make(g + slots_bytes(tiles), groups(tiles));
     return s;
   }
   __device__ __forceinline__ void publish(uint64_t t, uint32_t flag, T v) const {
     if constexpr (PACKED) {
-      static_assert(sizeof(T) == 4, "packed layout holds 4-byte values");
-      st_relaxed_u64(words + t, ((uint64_t)flag << 32) | to_bits64(v));
+      static_assert(StatePack<T>::kPackable, "value does not pack beside its flag");
+      st_relaxed_u64(words + t, StatePack<T>::pack(flag, v));
     } else {
       st_relaxed_any((flag == kFlagAgg ? agg : incl) + t, v);
       st_release_u32(flags + t, flag);
@@ -155,9 +221,7 @@ struct TileState {
   // Reads flag and the value it guards (aggregate for 1, inclusive for 2).
   __device__ __forceinline__ uint32_t peek(uint64_t t, T& v) const {
     if constexpr (PACKED) {
-      uint64_t w = ld_relaxed_u64(words + t);
-      v = from_bits64<T>(w & 0xFFFFFFFFull);
-      return (uint32_t)(w >> 32);
+      return StatePack<T>::unpack(ld_relaxed_u64(words + t), v);
     } else {
       uint32_t f = ld_acquire_u32(flags + t);
       if (f != kFlagNone) v = ld_relaxed_any((f == kFlagAgg ? agg : incl) + t);
@@ -266,6 +330,117 @@ __device__ T lookback_exclusive(const State& st, uint64_t tile, const OpT& op,
     }
     return acc;
   }
+}
+
+// Deterministic exclusive prefix of `tile` (tile >= 1) for non-associative
+// (floating-point) operators, executed by one full warp; `own` is the tile's
+// aggregate, already published with kFlagAgg (in this mode tiles publish no
+// inclusive prefix, except tile 0, whose inclusive prefix is its aggregate).
+// Tiles form groups of 32; the prefix is a fixed association of the
+// aggregates, whatever the timing:
+//
+//   H_g(k) = lane k of a warp inclusive scan (shuffle-up tree) over the
+//            aggregates of group g's tiles 0..k,
+//   A(g)   = H_g(31), published by the group's last tile,
+//   G(g)   = G(g-1) op A(g), G(0) = A(0), published by whichever tile first
+//            computes it (the same bits every time),
+//   E(32g + r) = G(g-1) op H_g(r-1)   (either term absent at g = 0 / r = 0).
+//
+// A tile waits only for its own group's predecessors and folds serially one
+// group aggregate per group back to the nearest published G, instead of one
+// tile aggregate per tile back to the nearest inclusive tile.
+template <class T, class OpT, class State>
+__device__ T lookback_grouped(const State& st, uint64_t tile, const OpT& op, DevErr err,
+                              T fallback, T own) {
+  const int lane = (int)lane_id();
+  SpinGuard guard(err.abort);
+  const uint64_t g = tile >> 5;
+  const int r = (int)(tile & 31);
+  T hs = fallback;
+  {
+    const bool valid = lane < r;
+    uint32_t f;
+    T v = fallback;
+    if (!wait_window<T>(st, (int64_t)(g << 5) + lane, valid, f, v, guard)) {
+      raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+      return fallback;
+    }
+    if (lane == r) v = own;
+    T x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      T y = shfl_up(x, d);
+      if (lane >= d) x = op(y, x);
+    }
+    if (r > 0) hs = shfl_idx(x, r - 1);
+    if (r == 31) {
+      const T a = shfl_idx(x, 31);
+      if (lane == 0) {
+        st.gagg.publish(g, a);
+        if (g == 0) st.gincl.publish(0, a);
+      }
+    }
+  }
+  if (g == 0) return hs;
+  // G(g-1): window by window back to the nearest group h with G(h); every
+  // group after it has its aggregate (a group's A is published before any G
+  // of it can be computed).
+  int64_t base = (int64_t)g - 1;
+  int64_t h = -1;
+  T gh = fallback;
+  while (true) {
+    const int64_t q = base - lane;
+    const bool valid = q >= 0;
+    T va = fallback, vi = fallback;
+    bool ha = false, hi = false;
+    while (true) {
+      if (valid) {  // both reads in flight together
+        hi = st.gincl.peek((uint64_t)q, vi);
+        ha = st.gagg.peek((uint64_t)q, va);
+        ha = ha || hi;
+      }
+      if (!__any_sync(kFull, valid && !ha)) break;
+      if (__any_sync(kFull, guard.expired())) {
+        raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+        return fallback;
+      }
+    }
+    const uint32_t m = __ballot_sync(kFull, valid && hi);
+    if (!m) {
+      if (base < 32) {
+        // This window reaches group 0, whose G follows its A: read again.
+        if (__any_sync(kFull, guard.expired())) {
+          raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+          return fallback;
+        }
+        continue;
+      }
+      base -= 32;
+      continue;
+    }
+    const int hl = __ffs(m) - 1;
+    h = base - hl;
+    gh = shfl_idx(vi, hl);
+    if (base == (int64_t)g - 1) {
+      // Found in the first window: the newer groups' aggregates are at hand.
+      T acc = gh;
+      for (int k = hl - 1; k >= 0; --k) acc = op(acc, shfl_idx(va, k));
+      if (lane == 0 && hl > 0) st.gincl.publish(g - 1, acc);
+      return r > 0 ? op(acc, hs) : acc;
+    }
+    break;
+  }
+  // Deeper: fold A(h+1) .. A(g-1) from fresh reads (all published).
+  T acc = gh;
+  for (int64_t c = h + 1; c < (int64_t)g; c += 32) {
+    const int64_t q = c + lane;
+    T va = fallback;
+    if (q < (int64_t)g) st.gagg.peek((uint64_t)q, va);
+    const int cnt = (int)min((int64_t)32, (int64_t)g - c);
+    for (int k = 0; k < cnt; ++k) acc = op(acc, shfl_idx(va, k));
+  }
+  if (lane == 0) st.gincl.publish(g - 1, acc);
+  return r > 0 ? op(acc, hs) : acc;
 }
 
 }  // namespace mb

@@ -102,6 +102,8 @@ __device__ __forceinline__ void tile_prefixes(uint64_t tile, const ScanParams<T>
     if (lane == 0) st.publish(0, kFlagIncl, agg);
   } else {
     if (lane == 0) st.publish(tile, kFlagAgg, agg);
+    // Floats: the fold-forward look-back (lookback.cuh); its per-tile
+    // inclusive prefixes keep the look-back short for these 32 KB tiles.
     excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.err, agg);
     if (lane == 0) st.publish(tile, kFlagIncl, op(excl, agg));
   }

@@ -10,9 +10,10 @@
 // by_key.rs:79-121 for reduce_by_key) with one kernel per call.
 //
 // Each tile marks its segment heads in a shared-memory bitmap -- from the
-// offsets (binary search for the tile's first segment, then one read per
-// segment start) or, for the by-key algorithms, from adjacent key
-// inequality -- and scans (head count, value) pairs under the segmented
+// offsets (the tile's first segment comes from a per-tile lower bound that a
+// small kernel computes for all tiles in parallel, then one read per segment
+// start) or, for the by-key algorithms, from adjacent key inequality -- and
+// scans (head count, value) pairs under the segmented
 // operator  (ha, a) . (hb, b) = (ha + hb, hb ? b : a op b),  which is
 // associative, so the decoupled look-back of lookback.cuh carries segment
 // boundaries across tiles.  Reductions stage the tile's inclusive pairs in
@@ -46,6 +47,26 @@ struct SegVal {
   V v;
 };
 
+}  // namespace
+
+// A (head count, 4-byte value) pair packs into one status word with its flag:
+// flag in bits 62-63, head count (below 2^30: at most one head per item) in
+// bits 32-61, value bits in 0-31 -- one load per predecessor in the look-back.
+template <class V>
+struct StatePack<SegVal<V>> {
+  static constexpr bool kPackable = sizeof(V) == 4;
+  __device__ __forceinline__ static uint64_t pack(uint32_t flag, const SegVal<V>& x) {
+    return ((uint64_t)flag << 62) | ((uint64_t)(x.heads & 0x3FFFFFFFu) << 32) | to_bits64(x.v);
+  }
+  __device__ __forceinline__ static uint32_t unpack(uint64_t w, SegVal<V>& x) {
+    x.heads = (uint32_t)(w >> 32) & 0x3FFFFFFFu;
+    x.v = from_bits64<V>(w & 0xFFFFFFFFull);
+    return (uint32_t)(w >> 62);
+  }
+};
+
+namespace {
+
 template <class V, int OP>
 struct SegOp {
   Op<V, OP> op;
@@ -74,6 +95,7 @@ struct SegParams {
   V init;
   const uint32_t* offsets;  // nseg + 1 entries
   uint64_t nseg;
+  const uint32_t* tile_lb;  // per tile t: first segment starting at or after t * TILE
   Src keys;
   void* out;
   void* out_keys;
@@ -110,6 +132,21 @@ __device__ __forceinline__ uint64_t upper_bound_u32(const uint32_t* a, uint64_t 
   return lo;
 }
 
+// tile_lb[t] = first s in [0, nseg] with offsets[s] >= t * tile, for every
+// tile t in [0, tiles]: one thread per offset s fills the tiles whose first
+// position lies in (offsets[s-1], offsets[s]] -- O(segments + tiles) work in
+// parallel, instead of a dependent binary search per tile.
+__global__ void __launch_bounds__(kThreads)
+    seg_tile_bounds_kernel(const uint32_t* __restrict__ offsets, uint64_t nseg, uint64_t tile,
+                           uint64_t tiles, uint32_t* __restrict__ tile_lb) {
+  for (uint64_t s = blockIdx.x * (uint64_t)kThreads + threadIdx.x; s <= nseg;
+       s += (uint64_t)gridDim.x * kThreads) {
+    const uint64_t lo = s == 0 ? 0 : (uint64_t)offsets[s - 1] / tile + 1;
+    const uint64_t hi = min((uint64_t)offsets[s] / tile, tiles);
+    for (uint64_t t = lo; t <= hi; ++t) tile_lb[t] = (uint32_t)s;
+  }
+}
+
 __device__ __forceinline__ void st_raw_bits(void* p, uint64_t i, int esize, uint64_t bits) {
   switch (esize) {
     case 1: ((uint8_t*)p)[i] = (uint8_t)bits; break;
@@ -119,9 +156,9 @@ __device__ __forceinline__ void st_raw_bits(void* p, uint64_t i, int esize, uint
   }
 }
 
-template <class V, int OP, bool PLAIN>
+template <class V, int OP, bool PLAIN, bool PK>
 __global__ void __launch_bounds__(kThreads)
-    seg_kernel(Src in, uint64_t cap, SegParams<V> p, TileState<SegVal<V>, false> st) {
+    seg_kernel(Src in, uint64_t cap, SegParams<V> p, TileState<SegVal<V>, PK> st) {
   using C = SegCfg<V>;
   using T = SegVal<V>;
   constexpr int VEC = C::VEC;
@@ -149,11 +186,11 @@ __global__ void __launch_bounds__(kThreads)
   // ---- heads ----
   if (p.heads_src == kHeadsOffsets) {
     if (tid == 0) {
-      const uint64_t cnt = p.nseg + 1;
-      const uint64_t sc = upper_bound_u32(p.offsets, cnt, tb) - 1;  // segment holding tb
-      const uint64_t sa = lower_bound_u32(p.offsets, cnt, tb);      // first start >= tb
-      const uint64_t sb = last_tile ? p.nseg : min(lower_bound_u32(p.offsets, cnt, te), p.nseg);
-      s_seg[0] = (sc < p.nseg && p.offsets[sc] < tb) ? sc : ~0ull;
+      const uint64_t sa = p.tile_lb[tile];  // first start >= tb
+      const uint64_t sb = last_tile ? p.nseg : min((uint64_t)p.tile_lb[tile + 1], p.nseg);
+      // The segment before sa holds tb (and continues into this tile)
+      // unless one starts exactly at tb.
+      s_seg[0] = (sa > 0 && p.offsets[sa] > tb) ? sa - 1 : ~0ull;
       s_seg[1] = sa;
       s_seg[2] = sb;
     }
@@ -173,11 +210,14 @@ __global__ void __launch_bounds__(kThreads)
                                     src_load_bits(p.keys, te))
                           : 1u;
       if (p.offsets) {  // segment starts are run heads too
-        const uint64_t cnt = p.nseg + 1;
-        s_seg[1] = lower_bound_u32(p.offsets, cnt, tb);
-        s_seg[2] = min(lower_bound_u32(p.offsets, cnt, te), p.nseg);
-        const uint64_t at = lower_bound_u32(p.offsets, cnt, te);
-        if (te < n && at < p.nseg && p.offsets[at] == te) h = 1u;
+        s_seg[1] = p.tile_lb[tile];
+        if (te < n) {
+          const uint64_t at = p.tile_lb[tile + 1];  // first start >= te
+          s_seg[2] = min(at, p.nseg);
+          if (at < p.nseg && p.offsets[at] == te) h = 1u;
+        } else {
+          s_seg[2] = p.nseg;
+        }
       }
       s_head_te = h;
     }
@@ -261,11 +301,14 @@ __global__ void __launch_bounds__(kThreads)
       if (lane == 0) st.publish(0, kFlagIncl, agg);
     } else {
       if (lane == 0) st.publish(tile, kFlagAgg, agg);
-      T excl = lookback_exclusive<T, SegOp<V, OP>, DET>(st, tile, op, p.err, agg);
-      if (lane == 0) {
-        st.publish(tile, kFlagIncl, op(excl, agg));
-        s_excl = excl;
+      T excl;
+      if constexpr (DET) {
+        excl = lookback_grouped<T>(st, tile, op, p.err, agg, agg);
+      } else {
+        excl = lookback_exclusive<T, SegOp<V, OP>, false>(st, tile, op, p.err, agg);
+        if (lane == 0) st.publish(tile, kFlagIncl, op(excl, agg));
       }
+      if (lane == 0) s_excl = excl;
     }
   }
   __syncthreads();
@@ -386,30 +429,49 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   memcpy(&p.init, init_wide, sizeof(V));
   const uint64_t tiles = (cap + C::TILE - 1) / C::TILE;
   using T = SegVal<V>;
-  const size_t state_b = TileState<T, false>::bytes(tiles);
+  // Packed states when the pair fits one word beside its flag.
+  const bool pk = StatePack<T>::kPackable && cap < (1ull << 30);
+  const size_t state_b =
+      pk ? TileState<T, true>::bytes(tiles) : TileState<T, false>::bytes(tiles);
+  const size_t lb_b = p.offsets ? ((tiles + 1) * 4 + 255) / 256 * 256 : 0;
   Scratch scratch;
-  MB_TRY(scratch.alloc(ex, 256 + state_b));
+  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b));
   MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + state_b, ex->stream));
   p.counter = scratch.as<uint32_t>();
   p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
-  auto st = TileState<T, false>::make(scratch.as<char>() + 256, tiles);
+  if (p.offsets) {
+    uint32_t* lb = (uint32_t*)(scratch.as<char>() + 256 + state_b);
+    MB_CUDA(cudaMemsetAsync(lb, 0xFF, (tiles + 1) * 4, ex->stream));
+    const uint64_t blocks = std::min<uint64_t>((p.nseg + kThreads) / kThreads, 4096);
+    seg_tile_bounds_kernel<<<(unsigned)std::max<uint64_t>(1, blocks), kThreads, 0, ex->stream>>>(
+        p.offsets, p.nseg, C::TILE, tiles, lb);
+    MB_CUDA(cudaGetLastError());
+    p.tile_lb = lb;
+  }
   const bool plain = src_plain(in, DTypeOf<V>::value) && (uintptr_t)in.data % 16 == 0 &&
                      (p.mode == kReduce || (uintptr_t)p.out % 16 == 0);
   const Src s = to_src(in);
   const size_t smem = seg_smem<V>(p.mode);
-#define MB_SEG_LAUNCH(OPID)                                                                    \
-  do {                                                                                         \
-    if (plain) {                                                                               \
-      auto k = seg_kernel<V, OPID, true>;                                                      \
-      if (smem > 48 * 1024)                                                                    \
-        MB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-      k<<<(unsigned)tiles, kThreads, smem, ex->stream>>>(s, cap, p, st);                       \
-    } else {                                                                                   \
-      auto k = seg_kernel<V, OPID, false>;                                                     \
-      if (smem > 48 * 1024)                                                                    \
-        MB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-      k<<<(unsigned)tiles, kThreads, smem, ex->stream>>>(s, cap, p, st);                       \
-    }                                                                                          \
+  char* state_base = scratch.as<char>() + 256;
+  auto launch = [&](auto kern, auto st) -> int {
+    if (smem > 48 * 1024)
+      MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)tiles, kThreads, smem, ex->stream>>>(s, cap, p, st);
+    return MB_OK;
+  };
+#define MB_SEG_LAUNCH(OPID)                                                           \
+  do {                                                                                \
+    if constexpr (StatePack<T>::kPackable) {                                          \
+      if (pk) {                                                                       \
+        auto st = TileState<T, true>::make(state_base, tiles);                        \
+        MB_TRY(plain ? launch(seg_kernel<V, OPID, true, true>, st)                     \
+                     : launch(seg_kernel<V, OPID, false, true>, st));                  \
+        break;                                                                        \
+      }                                                                               \
+    }                                                                                 \
+    auto st = TileState<T, false>::make(state_base, tiles);                           \
+    MB_TRY(plain ? launch(seg_kernel<V, OPID, true, false>, st)                        \
+                 : launch(seg_kernel<V, OPID, false, false>, st));                     \
   } while (0)
   switch (p.op) {
     case MB_OP_ADD: MB_SEG_LAUNCH(MB_OP_ADD); break;
