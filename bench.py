@@ -617,11 +617,18 @@ def time_steps(ex, wl, steps, warmup, dist, kernel_times=None):
         kernel_times["ms"] = float(kms.value)
     ex.sync()
     if dist:
-        import torch.distributed as D
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        D.all_reduce(t, op=D.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, "cuda")
     return ms
+
+
+def max_over_ranks(value: float, device: str) -> float:
+    """The largest `value` of all ranks (every rank takes part; the
+    whole job's time is its slowest rank's)."""
+    import torch
+    import torch.distributed as D
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    D.all_reduce(t, op=D.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cpu_baseline(wl, budget_s=12.0):

@@ -212,3 +212,27 @@ def test_kernel_timing_counts_onesweep_launches():
     cnt = C.c_uint64()
     L.mb_kernel_timing_read(ex.handle, N.KF_RADIX_ONESWEEP, C.byref(cnt), None)
     assert cnt.value == 0  # read forgets
+
+
+def test_autotune_records_and_selects_fastest(tmp_path):
+    """autotune times every radix shape on the caller's workload, persists
+    the fastest for (device, family, dtype, size bucket) and selects it; the
+    sort stays bit-exact under the chosen shape."""
+    import torch
+
+    from massively_b200 import _native as N, tune, vector
+    ex = executor()
+    n = 1 << 20
+    keys = seeded(np.uint32, n, 21)
+    vals = _perm_values(n)
+    dk, dv = ex.to_device(keys), ex.to_device(vals)
+    db = str(tmp_path / "tune.json")
+    best = tune.autotune(ex, "radix", "u32", n, lambda: vector.radix_sort_pairs(ex, dk, dv),
+                         reps=2, warmup=1, path=db)
+    assert 0 <= best < len(tune.configs("radix"))
+    assert N.lib().mb_tune_get(ex.handle, tune.FAMILIES["radix"]) == best
+    assert tune.lookup(torch.cuda.get_device_name(0), "radix", "u32", n, db) == best
+    sk, sv = vector.radix_sort_pairs(ex, dk, dv)
+    np.testing.assert_array_equal(ex.to_host(sv), orc.radix_perm([keys]))
+    tune.set_config(ex, "radix", -1)
+    ex.sync()
