@@ -448,7 +448,7 @@ struct OnesweepTmaSmem {
   uint64_t bar;
 };
 
-template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool FULL>
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool P64, bool FULL>
 __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>& sm,
                                               const uint32_t tile, const uint32_t valid,
                                               const int pass, const uint32_t n,
@@ -544,15 +544,40 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
   // Keys to their tile-sorted positions (in place: all were read above).
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) rd[k] = (rd[k] & 0xFFFFu) + sm.warp_cnt[warp][rd[k] >> 16];
-#pragma unroll
-  for (int k = 0; k < ITEMS; ++k)
-    if (FULL || wl + k * 32 < valid) sm.keys[rd[k]] = key[k];
+  // P64: 4-byte keys and values are staged as one 64-bit (value, key) word
+  // per item over the keys + values area (one store and one load per item
+  // instead of two each).
+  static_assert(!P64 || (sizeof(K) == 4 && sizeof(V) == 4), "P64 stages 4-byte pairs");
+  uint64_t* stage64 = reinterpret_cast<uint64_t*>(sm.keys);
   V val[KEYS_ONLY ? 1 : ITEMS];
-  if constexpr (!KEYS_ONLY) {
+  if constexpr (P64) {
+    // Two tile positions (below 2^16) per register, to hold keys, values and
+    // positions together in registers.
+    static_assert(ITEMS % 2 == 0, "positions are packed in pairs");
+    uint32_t pos2[ITEMS / 2];
+#pragma unroll
+    for (int k = 0; k < ITEMS; k += 2) pos2[k / 2] = rd[k] | (rd[k + 1] << 16);
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k) {
       const uint32_t li = wl + k * 32;
       val[k] = (FULL || li < valid) ? sm.vals[li] : V(0);
+    }
+    __syncthreads();  // every key and value of the tile is in registers
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k)
+      if (FULL || wl + k * 32 < valid)
+        stage64[(pos2[k / 2] >> (16 * (k & 1))) & 0xFFFFu] =
+            ((uint64_t)(uint32_t)val[k] << 32) | (uint32_t)key[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k)
+      if (FULL || wl + k * 32 < valid) sm.keys[rd[k]] = key[k];
+    if constexpr (!KEYS_ONLY) {
+#pragma unroll
+      for (int k = 0; k < ITEMS; ++k) {
+        const uint32_t li = wl + k * 32;
+        val[k] = (FULL || li < valid) ? sm.vals[li] : V(0);
+      }
     }
   }
 
@@ -589,7 +614,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
     }
     sm.delta[tid] = digit_offsets[pass * kBins + tid] + excl - sm.tile_start[tid];
   }
-  if constexpr (!KEYS_ONLY) {
+  if constexpr (!KEYS_ONLY && !P64) {
     __syncthreads();  // every original value is in registers
 #pragma unroll
     for (int k = 0; k < ITEMS; ++k)
@@ -603,18 +628,27 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
   for (int r = 0; r < ITEMS; ++r) {
     const uint32_t i = (uint32_t)r * THREADS + tid;
     if (!FULL && i >= valid) break;
-    const K kk = sm.keys[i];
+    K kk;
+    V vv{};
+    if constexpr (P64) {
+      const uint64_t kv = stage64[i];
+      kk = (K)(uint32_t)kv;
+      vv = (V)(uint32_t)(kv >> 32);
+    } else {
+      kk = sm.keys[i];
+    }
     const uint32_t o = sm.delta[digit_of<K, ENC>(kk, shift)] + i;
     if (o >= n) {  // only reachable after a failed look-back
       raise_device_error(err, MB_DEV_ERR_BOUNDS);
       continue;
     }
     __stcs(out_k + o, kk);
-    if constexpr (!KEYS_ONLY) __stcs(out_v + o, sm.vals[i]);
+    if constexpr (P64) __stcs(out_v + o, vv);
+    else if constexpr (!KEYS_ONLY) __stcs(out_v + o, sm.vals[i]);
   }
 }
 
-template <class K, int ENC, class V, int THREADS, int ITEMS, int NT>
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool P64>
 __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THREADS >= 384 ? 2 : 4) : 3)
     radix_onesweep_tma_kernel(const PassPlan* __restrict__ plan, int pass, uint32_t n,
                               const uint32_t* __restrict__ digit_offsets,
@@ -669,7 +703,7 @@ __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THRE
   V* out_v = (V*)plan->out_v[pass];
   if (valid == TILE) {
     if (!mbar_wait(&sm.bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, true>(sm, tile, valid, pass, n, digit_offsets,
+    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, P64, true>(sm, tile, valid, pass, n, digit_offsets,
                                                    status, err, out_k, out_v);
   } else {
     for (uint32_t i = tid; i < valid; i += THREADS) {
@@ -677,7 +711,7 @@ __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THRE
       if constexpr (!KEYS_ONLY) sm.vals[i] = in_v[tile_base + i];
     }
     __syncthreads();
-    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, false>(sm, tile, valid, pass, n, digit_offsets,
+    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, P64, false>(sm, tile, valid, pass, n, digit_offsets,
                                                     status, err, out_k, out_v);
   }
 }
@@ -694,11 +728,14 @@ constexpr RadixCfg kRadixCfgs[] = {
     {256, 12, "onesweep 256 threads x 12 keys (3072-key tiles), three peer-mask tables"},
     {1024, 16, "onesweep 1024 threads x 16 keys (16384-key tiles), one peer-mask table"},
     {384, 16, "onesweep 384 threads x 16 keys (6144-key tiles), one peer-mask table"},
+    {512, 16, "onesweep 512 threads x 16 keys, 4-byte pairs staged as one 64-bit word"},
+    {512, 12, "onesweep 512 threads x 12 keys (6144-key tiles), 64-bit pair staging"},
+    {384, 16, "onesweep 384 threads x 16 keys (6144-key tiles), 64-bit pair staging"},
 };
 constexpr int kRadixDefault = 0;    // 64-bit keys or values
-constexpr int kRadixDefault32 = 2;  // 32-bit keys, values of at most 32 bits
+constexpr int kRadixDefault32 = 6;  // 32-bit keys, values of at most 32 bits
 
-template <class K, int ENC, class V, int THREADS, int ITEMS, int NT = 1>
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT = 1, bool P64 = false>
 int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v,
                       uint64_t n, const uint32_t* n_dev) {
   constexpr int PASSES = (int)sizeof(K);
@@ -748,7 +785,8 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
                        (KEYS_ONLY || ((uintptr_t)in_v % 16 == 0 && (uintptr_t)out_v % 16 == 0));
   if (aligned) {
     const size_t smem = sizeof(OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>);
-    auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS, NT>;
+    auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS, NT,
+                                          P64 && sizeof(K) == 4 && sizeof(V) == 4>;
     MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int p = 0; p < PASSES; ++p) {
       {
@@ -786,6 +824,12 @@ int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* ou
     case 3: return onesweep_sort_cfg<K, ENC, V, 256, 12, 3>(ex, in_k, in_v, out_k, out_v, n, n_dev);
     case 4: return onesweep_sort_cfg<K, ENC, V, 1024, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
     case 5: return onesweep_sort_cfg<K, ENC, V, 384, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 6:
+      return onesweep_sort_cfg<K, ENC, V, 512, 16, 1, true>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 7:
+      return onesweep_sort_cfg<K, ENC, V, 512, 12, 1, true>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 8:
+      return onesweep_sort_cfg<K, ENC, V, 384, 16, 1, true>(ex, in_k, in_v, out_k, out_v, n, n_dev);
     default: return onesweep_sort_cfg<K, ENC, V, 256, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
   }
 }
