@@ -501,6 +501,57 @@ class GroupByC4(Workload):
         return self.alg_bytes() * n_gpus / (ms * 1e-3) / 1e9
 
 
+class SimpleWorkload(Workload):
+    """A one-call step over resident inputs, reported in GB/s of its byte
+    model: reduce (n * 4), merge of two sorted lists ((l + r) * 4 * 2),
+    gather through a random permutation (n * 12: indices, the values they
+    pick, the output)."""
+
+    kernel = "single call"
+
+    def __init__(self, kind, n):
+        self.kind, self.n = kind, n
+        lg = int(np.log2(n))
+        self.name = {"reduce": f"reduce_add_u32_2^{lg}", "merge": f"merge_u32_2x2^{lg - 1}",
+                     "gather": f"gather_u32_2^{lg}"}[kind]
+        self.metric = f"{kind} GB/s"
+        self.unit = "GB/s"
+        self.dtype = "u32"
+
+    def setup(self, ex):
+        from massively_b200 import lazy, vector
+        if self.kind == "reduce":
+            self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 8, self.n)
+        elif self.kind == "merge":
+            h = self.n // 2
+            self.a = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 9, h))
+            self.b = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 10, h))
+        else:
+            self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 11, self.n)
+            r = device_uniform_u32(ex, 0, 0xFFFFFFFF, 12, self.n)
+            iota = ex.alloc(np.uint32, self.n)
+            vector.copy(ex, lazy.counting(0).take(self.n), iota)
+            self.idx = vector.radix_sort_by_key(ex, r, iota)  # a random permutation
+
+    def step(self, ex):
+        from massively_b200 import op, vector
+        if self.kind == "reduce":
+            self.out = vector.reduce_to_device(ex, self.x, np.uint32(0), op.Add)
+        elif self.kind == "merge":
+            self.out = vector.merge(ex, self.a, self.b)
+        else:
+            self.out = vector.gather(ex, self.x, self.idx)
+
+    def units(self):
+        return self.alg_bytes()
+
+    def alg_bytes(self):
+        return {"reduce": 4.0, "merge": 8.0, "gather": 12.0}[self.kind] * self.n
+
+    def value_from_ms(self, ms, n_gpus):
+        return self.alg_bytes() * n_gpus / (ms * 1e-3) / 1e9
+
+
 def _n(default_log2: int) -> int:
     """Items of a workload: its configured size, or 2^MB_BENCH_LOG2N for
     small profiling captures of the same kernels."""
@@ -520,9 +571,13 @@ WORKLOADS = {
     "seg_reduce_f32": lambda: SegScanF32(n=_n(26), mode="reduce"),
     "seg_sort_u32": lambda: SegScanF32(n=_n(26), mode="sort"),
     "group_by": lambda: GroupByC4(n=_n(27)),
+    "reduce_u32": lambda: SimpleWorkload("reduce", _n(30)),
+    "merge_u32": lambda: SimpleWorkload("merge", _n(28)),
+    "gather_u32": lambda: SimpleWorkload("gather", _n(28)),
 }
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64",
-             "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by"]
+             "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by", "reduce_u32",
+             "merge_u32", "gather_u32"]
 
 
 # -------------------------------------------------------------- helpers --

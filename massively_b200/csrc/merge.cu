@@ -3,12 +3,14 @@
 //
 // Merge (massively/src/core/merge.rs:24-1230: a merge-path control kernel
 // of 64 threads x 4 items writing a permutation, then a separate apply pass
-// for the payload) becomes one kernel: every block finds its two merge-path
-// splits by binary search in global memory, stages its slice of both inputs
-// in shared memory, each thread finds its own split there and merges 8
-// outputs serially, and the block writes keys and payload columns with
-// coalesced stores.  Ties take the left element first (vector.rs:493-513 of
-// massively's oracle: the right element is taken only when strictly less).
+// for the payload) becomes two: a small kernel finds the merge-path split of
+// every tile boundary (all binary searches at once), then every block reads
+// its two splits, stages its slice of both inputs in shared memory, each
+// thread finds its own split there and merges kItems outputs serially (an
+// odd count, so the threads' strided shared-memory accesses fall in distinct
+// banks), and the block writes keys and payload columns with coalesced
+// stores.  Ties take the left element first (vector.rs:493-513 of massively's
+// oracle: the right element is taken only when strictly less).
 //
 // Set operations (massively/src/core/set.rs:14-401) keep massively's
 // occurrence-rank rule: the k-th copy of a value in one input is kept by
@@ -28,7 +30,7 @@ namespace mb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kItems = 8;
+constexpr int kItems = 9;  // odd: conflict-free strided shared-memory access
 constexpr int kTile = kThreads * kItems;
 constexpr int kMaxPay = 12;
 
@@ -41,17 +43,32 @@ __device__ __forceinline__ bool cmp_less(int less, T a, T b) {
   }
 }
 
+// The comparison with the predicate fixed at compile time (hot kernels).
+template <class T, int LESS>
+__device__ __forceinline__ bool cmp_ct(T a, T b) {
+  if constexpr (LESS == MB_GREATER) return b < a;
+  else if constexpr (LESS == MB_TOTAL_LESS) return radix_enc<T>(a) < radix_enc<T>(b);
+  else return a < b;
+}
+
+// Element i of an input: a direct load for plain columns of type T, the
+// lazy-view loader otherwise.
+template <class T, bool PLAIN>
+__device__ __forceinline__ T merge_load(const Src& s, uint64_t i) {
+  if constexpr (PLAIN) return ((const T*)s.data)[i];
+  else return src_load<T>(s, i);
+}
+
 // Number of left elements among the first d outputs of the stable merge.
-template <class T>
-__device__ uint64_t merge_path(const Src& L, const Src& R, uint64_t nl, uint64_t nr, uint64_t d,
-                               int less) {
+template <class T, int LESS, bool PLAIN>
+__device__ uint64_t merge_path(const Src& L, const Src& R, uint64_t nl, uint64_t nr, uint64_t d) {
   uint64_t lo = d > nr ? d - nr : 0;
   uint64_t hi = d < nl ? d : nl;
   while (lo < hi) {
     const uint64_t mid = (lo + hi) >> 1;
-    const T l = src_load<T>(L, mid);
-    const T r = src_load<T>(R, d - 1 - mid);
-    if (!cmp_less<T>(less, r, l)) lo = mid + 1;
+    const T l = merge_load<T, PLAIN>(L, mid);
+    const T r = merge_load<T, PLAIN>(R, d - 1 - mid);
+    if (!cmp_ct<T, LESS>(r, l)) lo = mid + 1;
     else hi = mid;
   }
   return lo;
@@ -76,10 +93,22 @@ __device__ __forceinline__ void st_raw_pay(void* p, uint64_t i, int esize, uint6
 
 constexpr uint32_t kFromRight = 0x80000000u;
 
-template <class T>
+// The merge-path split of every tile boundary, one thread per boundary (all
+// binary searches in flight together rather than one dependent search at the
+// start of each tile).
+template <class T, int LESS, bool PLAIN>
 __global__ void __launch_bounds__(kThreads)
-    merge_kernel(Src L, Src R, int less, void* out, int out_dtype, Payload pay,
-                 uint32_t* count_dev) {
+    merge_splits_kernel(Src L, Src R, uint64_t tiles, uint64_t* __restrict__ splits) {
+  const uint64_t nl = src_len(L), nr = src_len(R), n = nl + nr;
+  for (uint64_t b = blockIdx.x * (uint64_t)kThreads + threadIdx.x; b <= tiles;
+       b += (uint64_t)gridDim.x * kThreads)
+    splits[b] = merge_path<T, LESS, PLAIN>(L, R, nl, nr, min(b * (uint64_t)kTile, n));
+}
+
+template <class T, int LESS, bool PLAIN>
+__global__ void __launch_bounds__(kThreads)
+    merge_kernel(Src L, Src R, void* out, int out_dtype, Payload pay,
+                 uint32_t* count_dev, const uint64_t* __restrict__ splits) {
   __shared__ T s_keys[kTile];
   __shared__ T s_out[kTile];
   __shared__ uint32_t s_src[kTile];
@@ -89,13 +118,13 @@ __global__ void __launch_bounds__(kThreads)
   const uint64_t d0 = (uint64_t)blockIdx.x * kTile;
   if (d0 >= n) return;
   const uint64_t d1 = min(d0 + (uint64_t)kTile, n);
-  if (threadIdx.x < 2) s_split[threadIdx.x] = merge_path<T>(L, R, nl, nr, threadIdx.x ? d1 : d0, less);
+  if (threadIdx.x < 2) s_split[threadIdx.x] = splits[blockIdx.x + threadIdx.x];
   __syncthreads();
   const uint64_t i0 = s_split[0], i1 = s_split[1];
   const uint64_t j0 = d0 - i0, j1 = d1 - i1;
   const int la = (int)(i1 - i0), lb = (int)(j1 - j0);
-  for (int t = threadIdx.x; t < la; t += kThreads) s_keys[t] = src_load<T>(L, i0 + t);
-  for (int t = threadIdx.x; t < lb; t += kThreads) s_keys[la + t] = src_load<T>(R, j0 + t);
+  for (int t = threadIdx.x; t < la; t += kThreads) s_keys[t] = merge_load<T, PLAIN>(L, i0 + t);
+  for (int t = threadIdx.x; t < lb; t += kThreads) s_keys[la + t] = merge_load<T, PLAIN>(R, j0 + t);
   __syncthreads();
   const int total = la + lb;
   const int dt = min((int)threadIdx.x * kItems, total);
@@ -103,28 +132,36 @@ __global__ void __launch_bounds__(kThreads)
   int lo = dt > lb ? dt - lb : 0, hi = dt < la ? dt : la;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (!cmp_less<T>(less, s_keys[la + dt - 1 - mid], s_keys[mid])) lo = mid + 1;
+    if (!cmp_ct<T, LESS>(s_keys[la + dt - 1 - mid], s_keys[mid])) lo = mid + 1;
     else hi = mid;
   }
+  // Serial merge with the two heads in registers: one shared-memory read per
+  // output.
   int a = lo, b = dt - lo;
-  for (int k = 0; k < kItems && dt + k < total; ++k) {
-    bool take_right;
-    if (a >= la) take_right = true;
-    else if (b >= lb) take_right = false;
-    else take_right = cmp_less<T>(less, s_keys[la + b], s_keys[a]);
-    if (take_right) {
-      s_out[dt + k] = s_keys[la + b];
-      s_src[dt + k] = kFromRight | (uint32_t)b;
-      ++b;
-    } else {
-      s_out[dt + k] = s_keys[a];
-      s_src[dt + k] = (uint32_t)a;
+  T ka = a < la ? s_keys[a] : T(0);
+  T kb = b < lb ? s_keys[la + b] : T(0);
+  const bool pay_on = pay.ncols != 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (dt + k >= total) break;
+    const bool take_left = b >= lb || (a < la && !cmp_ct<T, LESS>(kb, ka));
+    s_out[dt + k] = take_left ? ka : kb;
+    if (pay_on) s_src[dt + k] = take_left ? (uint32_t)a : (kFromRight | (uint32_t)b);
+    if (take_left) {
       ++a;
+      ka = a < la ? s_keys[a] : ka;
+    } else {
+      ++b;
+      kb = b < lb ? s_keys[la + b] : kb;
     }
   }
   __syncthreads();
+  const bool same_type = out_dtype == DTypeOf<T>::value;
   for (int t = threadIdx.x; t < total; t += kThreads) {
-    if (out) st_cast<T>(out_dtype, out, d0 + t, s_out[t]);
+    if (out) {
+      if (same_type) __stcs((T*)out + d0 + t, s_out[t]);
+      else st_cast<T>(out_dtype, out, d0 + t, s_out[t]);
+    }
     if (pay.ncols) {
       const uint32_t s = s_src[t];
       const bool right = s & kFromRight;
@@ -181,15 +218,41 @@ unsigned grid_n(uint64_t n) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 16));
 }
 
+template <class T, int LESS, bool PLAIN>
+int merge_launch(mb_executor* ex, const mb_src& l, const mb_src& r, void* out, int out_dtype,
+                 const Payload& pay, uint32_t* count_dev) {
+  const uint64_t cap = l.len + r.len;
+  const uint64_t tiles = std::max<uint64_t>(1, (cap + kTile - 1) / kTile);
+  Scratch splits;
+  MB_TRY(splits.alloc(ex, (tiles + 1) * sizeof(uint64_t)));
+  const uint64_t sblocks = std::min<uint64_t>((tiles + kThreads) / kThreads, 4096);
+  merge_splits_kernel<T, LESS, PLAIN><<<(unsigned)sblocks, kThreads, 0, ex->stream>>>(
+      to_src(l), to_src(r), tiles, splits.as<uint64_t>());
+  MB_CUDA(cudaGetLastError());
+  merge_kernel<T, LESS, PLAIN><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
+      to_src(l), to_src(r), out, out_dtype, pay, count_dev, splits.as<uint64_t>());
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+template <class T, int LESS>
+int merge_less(mb_executor* ex, const mb_src& l, const mb_src& r, void* out, int out_dtype,
+               const Payload& pay, uint32_t* count_dev) {
+  const int ct = DTypeOf<T>::value;
+  if (src_plain(l, ct) && src_plain(r, ct))
+    return merge_launch<T, LESS, true>(ex, l, r, out, out_dtype, pay, count_dev);
+  return merge_launch<T, LESS, false>(ex, l, r, out, out_dtype, pay, count_dev);
+}
+
 template <class T>
 int merge_run(mb_executor* ex, const mb_src& l, const mb_src& r, int less, void* out,
               int out_dtype, const Payload& pay, uint32_t* count_dev) {
-  const uint64_t cap = l.len + r.len;
-  const uint64_t tiles = std::max<uint64_t>(1, (cap + kTile - 1) / kTile);
-  merge_kernel<T><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(to_src(l), to_src(r), less, out,
-                                                                out_dtype, pay, count_dev);
-  MB_CUDA(cudaGetLastError());
-  return MB_OK;
+  switch (less) {
+    case MB_GREATER: return merge_less<T, MB_GREATER>(ex, l, r, out, out_dtype, pay, count_dev);
+    case MB_TOTAL_LESS:
+      return merge_less<T, MB_TOTAL_LESS>(ex, l, r, out, out_dtype, pay, count_dev);
+    default: return merge_less<T, MB_LESS>(ex, l, r, out, out_dtype, pay, count_dev);
+  }
 }
 
 template <class T>
