@@ -161,7 +161,19 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
 constexpr int kSmemTile = 8192;  // 4-byte items per tile (32 KB)
 constexpr int kSmemItems = kSmemTile / kThreads;  // 32 per thread, warp-striped
 
-template <bool FUSED>
+// PRED >= 0: the fused predicate fixed at compile time (IS_TRUE, IS_FALSE,
+// IS_EVEN, IS_ODD on the 32 raw bits of a 4-byte integer column, where the
+// sign does not matter); -1 evaluates the run-time map.
+template <int PRED>
+__device__ __forceinline__ uint32_t fused_flag(int map, int dtype, uint32_t x) {
+  if constexpr (PRED == MB_UN_IS_TRUE) return x != 0;
+  else if constexpr (PRED == MB_UN_IS_FALSE) return x == 0;
+  else if constexpr (PRED == MB_UN_IS_EVEN) return (x & 1u) == 0;
+  else if constexpr (PRED == MB_UN_IS_ODD) return (x & 1u) != 0;
+  else return map_to<uint32_t>(map, dtype, x) != 0;
+}
+
+template <bool FUSED, int PRED>
 __global__ void __launch_bounds__(kThreads)
     select_smem_kernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ stencil,
                        uint32_t* __restrict__ out, uint64_t n, int fused_map, int in_dtype,
@@ -206,16 +218,25 @@ __global__ void __launch_bounds__(kThreads)
   const uint32_t* wv = buf + warp * 32 * kSmemItems;
   const uint32_t* ws = wv + kSmemTile;
   auto flag = [&](int k) -> bool {
-    const uint64_t i = tile_base + (uint64_t)warp * 32 * kSmemItems + k * 32 + lane;
-    if (i >= n) return false;
+    if (!full) {
+      const uint64_t i = tile_base + (uint64_t)warp * 32 * kSmemItems + k * 32 + lane;
+      if (i >= n) return false;
+    }
     uint32_t f;
-    if constexpr (FUSED) f = map_to<uint32_t>(fused_map, in_dtype, wv[k * 32 + lane]) != 0;
+    if constexpr (FUSED) f = fused_flag<PRED>(fused_map, in_dtype, wv[k * 32 + lane]);
     else f = ws[k * 32 + lane] != 0;
     return (f ^ invert) != 0;
   };
-  uint32_t wcount = 0;
+  // Each round's ballot is kept by lane k (kSmemItems == 32 rounds), so the
+  // write phase reuses it instead of evaluating the predicate again.
+  static_assert(kSmemItems == 32, "one ballot per lane");
+  uint32_t wcount = 0, my_ballot = 0;
 #pragma unroll 8
-  for (int k = 0; k < kSmemItems; ++k) wcount += __popc(__ballot_sync(kFull, flag(k)));
+  for (int k = 0; k < kSmemItems; ++k) {
+    const unsigned b = __ballot_sync(kFull, flag(k));
+    if (lane == k) my_ballot = b;
+    wcount += __popc(b);
+  }
   if (lane == 0) s_wcount[warp] = wcount;
   __syncthreads();
   if (warp == 0) {
@@ -241,9 +262,8 @@ __global__ void __launch_bounds__(kThreads)
   const unsigned lt = (1u << lane) - 1u;
 #pragma unroll 8
   for (int k = 0; k < kSmemItems; ++k) {
-    const bool f = flag(k);
-    const unsigned b = __ballot_sync(kFull, f);
-    if (f) out[run + __popc(b & lt)] = wv[k * 32 + lane];
+    const unsigned b = __shfl_sync(kFull, my_ballot, k);
+    if ((b >> lane) & 1u) out[run + __popc(b & lt)] = wv[k * 32 + lane];
     run += __popc(b);
   }
 }
@@ -318,8 +338,17 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
         MB_CUDA(cudaGetLastError());
         return MB_OK;
       };
-      if (p.fused) MB_TRY(launch(select_smem_kernel<true>));
-      else MB_TRY(launch(select_smem_kernel<false>));
+      const bool int4 = in[0].dtype == MB_U32 || in[0].dtype == MB_I32;
+      if (!p.fused) MB_TRY(launch(select_smem_kernel<false, -1>));
+      else if (int4 && stencil->map == MB_UN_IS_EVEN)
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_EVEN>));
+      else if (int4 && stencil->map == MB_UN_IS_ODD)
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_ODD>));
+      else if (int4 && stencil->map == MB_UN_IS_TRUE)
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_TRUE>));
+      else if (int4 && stencil->map == MB_UN_IS_FALSE)
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_FALSE>));
+      else MB_TRY(launch(select_smem_kernel<true, -1>));
     } else if (fast)
       select_kernel<true><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
     else
