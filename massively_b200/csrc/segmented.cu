@@ -552,13 +552,6 @@ __global__ void offsets_from_prefix_kernel(const uint64_t* prefix, uint64_t nseg
   }
 }
 
-__global__ void segment_ids_kernel(const uint32_t* off, uint64_t nseg, uint32_t* ids, uint64_t n) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    ids[i] = (uint32_t)(upper_bound_u32(off, nseg + 1, i) - 1);
-  }
-}
-
 __global__ void lengths_kernel(const uint32_t* off, uint64_t nseg, uint32_t* len) {
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
        s += (uint64_t)gridDim.x * blockDim.x)
@@ -570,6 +563,87 @@ __global__ void local_indices_kernel(const uint32_t* off, uint64_t nseg, uint32_
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
     local[i] = (uint32_t)(i - off[upper_bound_u32(off, nseg + 1, i) - 1]);
+}
+
+// Segment ids of a chunk of kIdTile items per block, without a search per
+// item: the chunk's segment starts (from the per-tile lower bounds) are
+// counted per position in shared memory and scanned, so id(i) = (first
+// segment starting in the chunk) - 1 + starts at or before i.  COMP writes
+// the sort key (id << 32) | enc(value) of a 4-byte value instead of the id:
+// enc orders unsigned (0), signed (1) or float (2, total order) bits as
+// unsigned, complemented when `desc`; with `ieee`, -0 counts as +0.
+constexpr int kIdItems = 16;
+constexpr int kIdTile = kThreads * kIdItems;
+
+template <bool COMP>
+__global__ void __launch_bounds__(kThreads)
+    seg_ids_kernel(const uint32_t* __restrict__ off, uint64_t nseg, uint64_t n,
+                   const uint32_t* __restrict__ tile_lb, uint32_t* __restrict__ ids, Src values,
+                   int enc, int desc, int ieee, uint64_t* __restrict__ comp) {
+  __shared__ uint32_t cnt[kIdTile];
+  __shared__ uint32_t wsum[kWarps];
+  const uint64_t c0 = (uint64_t)blockIdx.x * kIdTile;
+  if (c0 >= n) return;
+  const uint64_t c1 = min(c0 + (uint64_t)kIdTile, n);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < kIdTile; i += kThreads) cnt[i] = 0;
+  __syncthreads();
+  const uint64_t lb = tile_lb[blockIdx.x];  // first s with off[s] >= c0
+  const uint64_t lbn = c1 < n ? (uint64_t)tile_lb[blockIdx.x + 1] : nseg + 1;
+  for (uint64_t sg = max(lb, (uint64_t)1) + tid; sg < lbn; sg += kThreads) {
+    const uint64_t o = off[sg];
+    if (o < c1) atomicAdd(&cnt[o - c0], 1u);
+  }
+  __syncthreads();
+  // Warp w scans positions [512 w, 512 w + 512) in rounds of 32.
+  uint32_t carry = 0;
+  uint32_t loc[kIdItems];
+#pragma unroll
+  for (int k = 0; k < kIdItems; ++k) {
+    uint32_t v = cnt[warp * 32 * kIdItems + k * 32 + lane];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, v, d);
+      if (lane >= d) v += o;
+    }
+    loc[k] = carry + v;
+    carry += __shfl_sync(kFull, v, 31);
+  }
+  if (lane == 0) wsum[warp] = carry;
+  __syncthreads();
+  uint32_t base = lb >= 1 ? (uint32_t)(lb - 1) : 0u;
+  for (int w = 0; w < warp; ++w) base += wsum[w];
+#pragma unroll
+  for (int k = 0; k < kIdItems; ++k) {
+    const uint64_t i = c0 + (uint64_t)warp * 32 * kIdItems + k * 32 + lane;
+    if (i >= c1) break;
+    const uint32_t id = base + loc[k];
+    if constexpr (COMP) {
+      uint32_t u = (uint32_t)src_load_bits(values, i);
+      if (ieee && (u & 0x7FFFFFFFu) == 0) u = 0;  // -0 == +0 under `<`
+      if (enc == 1) u ^= 0x80000000u;
+      else if (enc == 2) u = (u & 0x80000000u) ? ~u : (u ^ 0x80000000u);
+      if (desc) u = ~u;
+      comp[i] = ((uint64_t)id << 32) | u;
+    } else {
+      ids[i] = id;
+    }
+  }
+}
+
+// Inverse of the COMP encoding: the low 32 bits of a sorted key back to the
+// value's bits.
+__global__ void __launch_bounds__(kThreads)
+    seg_decode_kernel(const uint64_t* __restrict__ comp, uint64_t n, int enc, int desc,
+                      uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * kThreads) {
+    uint32_t u = (uint32_t)comp[i];
+    if (desc) u = ~u;
+    if (enc == 1) u ^= 0x80000000u;
+    else if (enc == 2) u = (u & 0x80000000u) ? (u ^ 0x80000000u) : ~u;
+    out[i] = u;
+  }
 }
 
 // ids must be non-decreasing and < nseg; bad[0] is set otherwise.
@@ -613,6 +687,41 @@ int check_values_out(mb_executor* ex, const mb_src* values, const mb_col& out, u
 }
 
 }  // namespace
+
+// Segment ids (ids != null) or the composite sort keys of a 4-byte value
+// column (comp != null) for `n` items over canonical offsets.
+int seg_ids_fill(mb_executor* ex, const uint32_t* offsets, uint64_t nseg, uint64_t n,
+                 uint32_t* ids, const mb_src* values, int enc, int desc, int ieee,
+                 uint64_t* comp) {
+  if (n == 0) return MB_OK;
+  const uint64_t tiles = (n + kIdTile - 1) / kIdTile;
+  Scratch lb;
+  MB_TRY(lb.alloc(ex, (tiles + 1) * 4));
+  MB_CUDA(cudaMemsetAsync(lb.ptr, 0xFF, (tiles + 1) * 4, ex->stream));
+  const uint64_t blocks = std::min<uint64_t>((nseg + kThreads) / kThreads, 4096);
+  seg_tile_bounds_kernel<<<(unsigned)std::max<uint64_t>(1, blocks), kThreads, 0, ex->stream>>>(
+      offsets, nseg, kIdTile, tiles, lb.as<uint32_t>());
+  MB_CUDA(cudaGetLastError());
+  const Src v = values ? to_src(*values) : Src{};
+  if (comp)
+    seg_ids_kernel<true><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
+        offsets, nseg, n, lb.as<uint32_t>(), nullptr, v, enc, desc, ieee, comp);
+  else
+    seg_ids_kernel<false><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
+        offsets, nseg, n, lb.as<uint32_t>(), ids, v, 0, 0, 0, nullptr);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int seg_decode_u32(mb_executor* ex, const uint64_t* comp, uint64_t n, int enc, int desc,
+                   uint32_t* out) {
+  if (n == 0) return MB_OK;
+  const unsigned g = (unsigned)std::min<uint64_t>((n + kThreads - 1) / kThreads, 148ull * 16);
+  seg_decode_kernel<<<g, kThreads, 0, ex->stream>>>(comp, n, enc, desc, out);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
 }  // namespace mb
 
 using namespace mb;
@@ -678,10 +787,7 @@ int mb_segmentation_segment_ids(mb_executor* ex, const uint32_t* offsets, uint64
                                 uint32_t* ids, uint64_t value_count) {
   MB_TRY(check_exec(ex));
   if (value_count == 0) return MB_OK;
-  segment_ids_kernel<<<grid_for_n(value_count), 256, 0, ex->stream>>>(offsets, segment_count, ids,
-                                                                     value_count);
-  MB_CUDA(cudaGetLastError());
-  return MB_OK;
+  return seg_ids_fill(ex, offsets, segment_count, value_count, ids, nullptr, 0, 0, 0, nullptr);
 }
 
 int mb_segmentation_lengths(mb_executor* ex, const uint32_t* offsets, uint64_t segment_count,

@@ -35,6 +35,11 @@ int radix_sort_plain(mb_executor* ex, int kdt, const void* ik, const void* iv, v
 int gather_raw(mb_executor* ex, const void* src, size_t esize, uint64_t nsrc,
                const uint32_t* idx, uint64_t n, void* dst, const uint32_t* n_dev = nullptr);
 int materialize(mb_executor* ex, const mb_src& in, void* dst);
+int seg_ids_fill(mb_executor* ex, const uint32_t* offsets, uint64_t nseg, uint64_t n,
+                 uint32_t* ids, const mb_src* values, int enc, int desc, int ieee,
+                 uint64_t* comp);
+int seg_decode_u32(mb_executor* ex, const uint64_t* comp, uint64_t n, int enc, int desc,
+                   uint32_t* out);
 
 namespace {
 
@@ -267,6 +272,35 @@ int mb_seg_sort(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
   if (less < MB_LESS || less > MB_TOTAL_LESS)
     return set_error(MB_ERR_LAUNCH, "seg sort takes LESS, GREATER or TOTAL_LESS");
   if (n == 0) return MB_OK;
+  const int vt = values->vtype;
+  if (dtype_size(vt) == 4 && dtype_size(out.dtype) == 4 && (vt == MB_U32 || vt == MB_I32 ||
+                                                            vt == MB_F32)) {
+    // 4-byte values: one radix sort of 64-bit keys (segment id << 32 |
+    // order-preserving bits of the value); the id's constant high digits
+    // are skipped by the onesweep plan.  Where the encoding is a bijection
+    // the sorted keys decode back to the values; under `<` / `>` on floats
+    // (-0 and +0 tie) the original bits ride along as the sort's values.
+    int ieee = 0, desc = 0;
+    comparator_mode(less, vt, &ieee, &desc);
+    const int enc = vt == MB_U32 ? 0 : vt == MB_I32 ? 1 : 2;
+    Scratch comp, sorted;
+    MB_TRY(comp.alloc(ex, n * 8));
+    MB_TRY(sorted.alloc(ex, n * 8));
+    MB_TRY(seg_ids_fill(ex, offsets, segment_count, n, nullptr, values, enc, desc, ieee,
+                        comp.as<uint64_t>()));
+    if (!ieee) {
+      MB_TRY(radix_sort_plain(ex, MB_U64, comp.ptr, nullptr, sorted.ptr, nullptr, 0, n));
+      return seg_decode_u32(ex, sorted.as<uint64_t>(), n, enc, desc, (uint32_t*)out.data);
+    }
+    const void* raw = values->data;
+    Scratch mat;
+    if (!is_plain_column(*values)) {
+      MB_TRY(mat.alloc(ex, n * 4));
+      MB_TRY(materialize(ex, *values, mat.ptr));
+      raw = mat.ptr;
+    }
+    return radix_sort_plain(ex, MB_U64, comp.ptr, raw, sorted.ptr, out.data, 4, n);
+  }
   Scratch ids, ids_out;
   MB_TRY(ids.alloc(ex, n * 4));
   MB_TRY(ids_out.alloc(ex, n * 4));
