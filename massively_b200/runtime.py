@@ -242,6 +242,20 @@ class Executor:
         out = vec.tensor[:n].cpu()
         return out.view(torch.uint8).numpy().view(vec.dtype) if n else np.empty(0, vec.dtype)
 
+    def reserve_pool(self, nbytes: int) -> None:
+        """Grows the device's stream-ordered pool to hold `nbytes` (capped
+        at 90% of free memory) by allocating and freeing one block: later
+        allocations up to that size reuse reserved memory instead of growing
+        the pool in the middle of the work (a slow driver path)."""
+        free, _ = torch.cuda.mem_get_info(self.device)
+        n = int(min(nbytes, free * 0.9))
+        if n <= 0:
+            return
+        with torch.cuda.device(self.device):
+            t = torch.empty(n, dtype=torch.uint8, device=f"cuda:{self.device}")
+            del t
+            torch.cuda.synchronize(self.device)
+
     def pool_stats(self) -> tuple[int, int]:
         used, res = C.c_uint64(), C.c_uint64()
         check(self._lib.mb_pool_stats(self._h, C.byref(used), C.byref(res)))

@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import math
 import time
+from collections import deque
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -213,12 +214,25 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
     GPU is busy therefore accumulate into larger batches.  A launch is
     admitted only while the bytes of everything in flight stay within
     `budget_bytes`; requests retire when their completion event fires."""
+    exec.reserve_pool(budget_bytes)
     pool = [torch.cuda.Stream() for _ in range(streams)]
     clock = _Clock()
-    waiting: list[Request] = []
+    # The queue in arrival order, plus one queue of small requests per kind
+    # (a request leaves both when launched; the other copy is skipped
+    # later), so forming a launch costs O(batch), not O(queue).
+    queue: deque[Request] = deque()
+    small: dict[str, deque[Request]] = {SORT: deque(), SCAN: deque(), RBK: deque()}
+    taken: set[int] = set()
+    nwait = 0
     inflight = []               # (event, [requests], bytes, stream index)
     load = [0] * streams        # launches in flight per stream
     used = max_used = launches = nxt = done_count = 0
+
+    def pop_live(q):
+        while q and q[0].rid in taken:
+            q.popleft()
+        return q[0] if q else None
+
     while done_count < len(reqs):
         still = []
         for ev, group, b, si in inflight:
@@ -237,29 +251,38 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
         inflight = still
         now = clock.now()
         while nxt < len(reqs) and reqs[nxt].arrival <= now:
-            waiting.append(reqs[nxt])
+            r = reqs[nxt]
+            queue.append(r)
+            if r.n <= small_n:
+                small[r.kind].append(r)
+            nwait += 1
             nxt += 1
         launched = False
-        while waiting:
+        while nwait:
             si = min(range(streams), key=lambda i: load[i])
             if load[si] >= depth:
                 break
-            head = waiting[0]
+            head = pop_live(queue)
             if head.n > small_n:
                 group = [head]
             else:
-                group, room = [], budget_bytes - used
-                for r in waiting:
-                    if r.kind == head.kind and r.n <= small_n and len(group) < max_batch:
-                        if r.bytes_needed() > room and group:
-                            break
-                        group.append(r)
-                        room -= r.bytes_needed()
+                group, room, q = [], budget_bytes - used, small[head.kind]
+                while len(group) < max_batch:
+                    r = pop_live(q)
+                    if r is None or (r.bytes_needed() > room and group):
+                        break
+                    q.popleft()
+                    group.append(r)
+                    room -= r.bytes_needed()
             b = sum(r.bytes_needed() for r in group)
             if used + b > budget_bytes and inflight:
+                if len(group) > 1 or head.n <= small_n:
+                    for r in reversed(group):  # back to the front of its queue
+                        small[head.kind].appendleft(r)
                 break               # wait for memory to come back
-            ids = {id(r) for r in group}
-            waiting = [r for r in waiting if id(r) not in ids]
+            for r in group:
+                taken.add(r.rid)
+            nwait -= len(group)
             with torch.cuda.stream(pool[si]):
                 exec.bind_current_stream()
                 if len(group) == 1:
@@ -276,7 +299,7 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
             launched = True
             inflight.append((ev, group, b, si))
         if not launched:
-            if not inflight and not waiting and nxt < len(reqs):
+            if not inflight and not nwait and nxt < len(reqs):
                 time.sleep(max(0.0, min(1e-3, reqs[nxt].arrival - clock.now())))
             elif inflight:
                 time.sleep(20e-6)
@@ -292,6 +315,7 @@ def plain_dispatch(exec: Executor, reqs: list[Request], keep_outputs: bool = Fal
     (plain request/response serving) each request's result is waited for
     before the next request is dispatched; without it the requests are
     queued back to back on the stream, with no coalescing or overlap."""
+    exec.reserve_pool(40 << 30)
     clock = _Clock()
     events = []
     for r in reqs:
