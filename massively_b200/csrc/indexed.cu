@@ -43,6 +43,46 @@ __global__ void __launch_bounds__(kThreads) copy_view_kernel(Src in, void* out, 
   for (; i < n; i += step) st_cast<T>(out_dtype, out, i, src_load<T>(in, i));
 }
 
+// The same for a 4-byte output of the view's own compute type, 16-byte
+// aligned: four items per thread and one 16-byte store (views such as
+// counting, constant or repeat_each compute their items, so stores dominate).
+// KIND: MB_SRC_COUNTING / MB_SRC_STRIDE of the output's own type with no map
+// (the item's bits are a + i*b, computed inline), or -1 for any view.
+template <class T, int KIND>
+__device__ __forceinline__ T view_item(const Src& in, uint64_t i) {
+  if constexpr (KIND == MB_SRC_COUNTING) {
+    const uint32_t b = (uint32_t)(in.a + i);
+    T x;
+    memcpy(&x, &b, 4);
+    return x;
+  } else if constexpr (KIND == MB_SRC_STRIDE) {
+    const uint32_t b = (uint32_t)(in.a + i * in.b);
+    T x;
+    memcpy(&x, &b, 4);
+    return x;
+  } else {
+    return src_load<T>(in, i);
+  }
+}
+
+template <class T, int KIND>
+__global__ void __launch_bounds__(kThreads) copy_view4_kernel(Src in, uint4* out, uint64_t n) {
+  static_assert(sizeof(T) == 4, "4-byte items");
+  const uint64_t nvec = n / 4;
+  uint64_t v = blockIdx.x * (uint64_t)kThreads + threadIdx.x;
+  const uint64_t step = (uint64_t)gridDim.x * kThreads;
+  for (; v < nvec; v += step) {
+    T x[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) x[k] = view_item<T, KIND>(in, 4 * v + k);
+    uint4 u;
+    memcpy(&u, x, 16);
+    __stcs(out + v, u);
+  }
+  for (uint64_t i = nvec * 4 + blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n; i += step)
+    reinterpret_cast<T*>(out)[i] = view_item<T, KIND>(in, i);
+}
+
 // 16-byte vector copy of a plain column (same element type both sides).
 __global__ void __launch_bounds__(kThreads) copy_vec_kernel(const uint4* in, uint4* out,
                                                             uint64_t nvec) {
@@ -152,6 +192,22 @@ uint32_t seed_key(uint64_t seed) {
 template <class T>
 int copy_run(mb_executor* ex, const mb_src& in, const mb_col& out) {
   const uint64_t n = in.len;
+  if constexpr (sizeof(T) == 4) {
+    if (out.dtype == DTypeOf<T>::value && (uintptr_t)out.data % 16 == 0 && !in.len_dev) {
+      const unsigned g = stride_grid((n + 3) / 4);
+      const bool own = in.map == MB_UN_IDENTITY && in.vtype == out.dtype && in.dtype == out.dtype;
+      if (own && in.kind == MB_SRC_COUNTING)
+        copy_view4_kernel<T, MB_SRC_COUNTING><<<g, kThreads, 0, ex->stream>>>(to_src(in),
+                                                                           (uint4*)out.data, n);
+      else if (own && in.kind == MB_SRC_STRIDE)
+        copy_view4_kernel<T, MB_SRC_STRIDE><<<g, kThreads, 0, ex->stream>>>(to_src(in),
+                                                                         (uint4*)out.data, n);
+      else
+        copy_view4_kernel<T, -1><<<g, kThreads, 0, ex->stream>>>(to_src(in), (uint4*)out.data, n);
+      MB_CUDA(cudaGetLastError());
+      return MB_OK;
+    }
+  }
   copy_view_kernel<T><<<stride_grid(n), kThreads, 0, ex->stream>>>(to_src(in), out.data,
                                                                     out.dtype, n);
   MB_CUDA(cudaGetLastError());
