@@ -204,7 +204,7 @@ class _Clock:
 
 
 def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
-          small_n: int = 1 << 20, max_batch: int = 256, streams: int = 4, depth: int = 2,
+          small_n: int = 1 << 20, max_batch: int = 256, streams: int = 8, depth: int = 4,
           keep_outputs: bool = False) -> ServeStats:
     """Continuous batching.  Arrived requests wait in a queue; whenever one
     of the `streams` launch slots (each holds up to `depth` launches in
