@@ -51,9 +51,12 @@ struct ScanCfg {
 
 template <class T>
 struct SmemCfg {
+  // Floats take 64 KB tiles: their deterministic look-back folds one
+  // aggregate per tile in sequence, so fewer, larger tiles shorten that chain.
+  static constexpr int ROWS = std::is_floating_point<T>::value ? 2 * kRows : kRows;
   static constexpr int VEC = 16 / sizeof(T);
-  static constexpr int WARP_ITEMS = 32 * kRows * VEC;
-  static constexpr int TILE = kWarps * WARP_ITEMS;  // 32 KB
+  static constexpr int WARP_ITEMS = 32 * ROWS * VEC;
+  static constexpr int TILE = kWarps * WARP_ITEMS;  // 32 KB (64 KB for floats)
   static constexpr int TILE_BYTES = TILE * (int)sizeof(T);
 };
 
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(kThreads)
   T* wb = buf + warp * C::WARP_ITEMS;
   T carry = T(0);
 #pragma unroll 2
-  for (int j = 0; j < kRows; ++j) {
+  for (int j = 0; j < C::ROWS; ++j) {
     T v[VEC];
     uint4 u = *reinterpret_cast<const uint4*>(wb + (j * 32 + lane) * VEC);
     memcpy(v, &u, 16);
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool has = s_has[warp];
   const uint64_t wg = tile_base + (uint64_t)warp * C::WARP_ITEMS;
 #pragma unroll 2
-  for (int j = 0; j < kRows; ++j) {
+  for (int j = 0; j < C::ROWS; ++j) {
     const int li = (j * 32 + lane) * VEC;  // warp-local index of item 0
     T v[VEC];
     uint4 u = *reinterpret_cast<const uint4*>(wb + li);
@@ -413,6 +416,9 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
 #define MB_SCAN_LAUNCH(OPID)                                                                    \
   do {                                                                                          \
     if (smem_path) {                                                                            \
+      if (smem > 48 * 1024)                                                                     \
+        MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED>,                         \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
       scan_smem_kernel<T, OPID, PACKED><<<grid, block, smem, ex->stream>>>(                     \
           (const T*)in.data, (T*)out.data, cap, p, st);                                         \
     } else if (plain) {                                                                         \
@@ -534,6 +540,9 @@ int scan_noalloc_run(mb_executor* ex, const mb_src& in, int op, const mb_col& ou
 #define MB_SCAN_NOALLOC_LAUNCH(OPID)                                                            \
   do {                                                                                          \
     if (smem_path) {                                                                            \
+      if (smem > 48 * 1024)                                                                     \
+        MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED>,                         \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
       scan_smem_kernel<T, OPID, PACKED><<<grid, block, smem, ex->stream>>>(                     \
           (const T*)in.data, (T*)out.data, cap, p, st);                                         \
     } else if (plain) {                                                                         \
