@@ -37,6 +37,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kLoads = 4;
+// Blocks per SM the segmented kernel is compiled for: at the compiler's
+// natural 123 registers only two fit, and warps sit at the barrier while
+// warp 0 looks back.
+constexpr int kSegMinBlocks = 4;
 
 enum SegMode : int { kScanIncl = 0, kScanExcl = 1, kReduce = 2 };
 enum HeadsSrc : int { kHeadsOffsets = 0, kHeadsKeys = 1 };
@@ -157,7 +161,7 @@ __device__ __forceinline__ void st_raw_bits(void* p, uint64_t i, int esize, uint
 }
 
 template <class V, int OP, bool PLAIN, bool PK>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kSegMinBlocks)
     seg_kernel(Src in, uint64_t cap, SegParams<V> p, TileState<SegVal<V>, PK> st) {
   using C = SegCfg<V>;
   using T = SegVal<V>;
