@@ -513,7 +513,8 @@ class SimpleWorkload(Workload):
         self.kind, self.n = kind, n
         lg = int(np.log2(n))
         self.name = {"reduce": f"reduce_add_u32_2^{lg}", "merge": f"merge_u32_2x2^{lg - 1}",
-                     "gather": f"gather_u32_2^{lg}"}[kind]
+                     "gather": f"gather_u32_2^{lg}",
+                     "lower_bound": f"lower_bound_u32_2^{lg}_in_2^24"}[kind]
         self.metric = f"{kind} GB/s"
         self.unit = "GB/s"
         self.dtype = "u32"
@@ -526,6 +527,9 @@ class SimpleWorkload(Workload):
             h = self.n // 2
             self.a = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 9, h))
             self.b = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 10, h))
+        elif self.kind == "lower_bound":
+            self.src = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 13, 1 << 24))
+            self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 14, self.n)
         else:
             self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 11, self.n)
             r = device_uniform_u32(ex, 0, 0xFFFFFFFF, 12, self.n)
@@ -539,6 +543,8 @@ class SimpleWorkload(Workload):
             self.out = vector.reduce_to_device(ex, self.x, np.uint32(0), op.Add)
         elif self.kind == "merge":
             self.out = vector.merge(ex, self.a, self.b)
+        elif self.kind == "lower_bound":
+            self.out = vector.lower_bound(ex, self.src, self.x)
         else:
             self.out = vector.gather(ex, self.x, self.idx)
 
@@ -546,7 +552,9 @@ class SimpleWorkload(Workload):
         return self.alg_bytes()
 
     def alg_bytes(self):
-        return {"reduce": 4.0, "merge": 8.0, "gather": 12.0}[self.kind] * self.n
+        # lower_bound: each query's value in and index out (the 64 MB source
+        # stays in L2 after the first probes)
+        return {"reduce": 4.0, "merge": 8.0, "gather": 12.0, "lower_bound": 8.0}[self.kind] * self.n
 
     def value_from_ms(self, ms, n_gpus):
         return self.alg_bytes() * n_gpus / (ms * 1e-3) / 1e9
@@ -574,10 +582,11 @@ WORKLOADS = {
     "reduce_u32": lambda: SimpleWorkload("reduce", _n(30)),
     "merge_u32": lambda: SimpleWorkload("merge", _n(28)),
     "gather_u32": lambda: SimpleWorkload("gather", _n(28)),
+    "lower_bound_u32": lambda: SimpleWorkload("lower_bound", _n(26)),
 }
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64",
              "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by", "reduce_u32",
-             "merge_u32", "gather_u32"]
+             "merge_u32", "gather_u32", "lower_bound_u32"]
 
 
 # -------------------------------------------------------------- helpers --

@@ -323,6 +323,16 @@ int mb_exclusive_scan_by_key(mb_executor* exec, const mb_src* keys, int key_eq,
 
 /* --------------------------------------------------------- merge / set ---- */
 
+/* vector::lower_bound / vector::upper_bound (massively/src/api/algorithm/
+ * search.rs:81-147): for every value, the partition point of the sorted
+ * `source` under `less` -- the first index whose element is not less than the
+ * value (lower) or that the value is less than (upper).  `out` receives one
+ * MIndex (u32) per value. */
+int mb_lower_bound(mb_executor* exec, const mb_src* source, const mb_src* values, int less,
+                   mb_col out);
+int mb_upper_bound(mb_executor* exec, const mb_src* source, const mb_src* values, int less,
+                   mb_col out);
+
 /* vector::merge (massively/src/api/algorithm/merge.rs:109; core
  * massively/src/core/merge.rs:24-1230): stable merge, left first on ties. */
 int mb_merge(mb_executor* exec, const mb_src* left, const mb_src* right, int less, mb_col out);

@@ -476,6 +476,31 @@ def exclusive_scan_by_key(exec: Executor, keys, values, equal, init, op):
 
 # ---------------------------------------------------------- merge / set --
 
+def _bounds(exec, source, values, less, fn):
+    _check_owner(exec, source, values)
+    keep = []
+    ss, vs = lower(exec, source, keep), lower(exec, values, keep)
+    _len(source)
+    out = exec.alloc(np.uint32, _len(values))
+    ld = _len_dev_of(values)
+    if ld is not None:
+        out = out.with_len_dev(ld)
+    check(fn(exec.handle, C.byref(ss), C.byref(vs), O.pred2(less).id, out.to_col()))
+    return out
+
+
+def lower_bound(exec: Executor, source, values, less=O.Less) -> DeviceVec:
+    """vector::lower_bound (massively/src/api/algorithm/search.rs:81): per
+    value, the first index of the sorted source not less than it."""
+    return _bounds(exec, source, values, less, _L().mb_lower_bound)
+
+
+def upper_bound(exec: Executor, source, values, less=O.Less) -> DeviceVec:
+    """vector::upper_bound (search.rs:128): per value, the first index of
+    the sorted source greater than it."""
+    return _bounds(exec, source, values, less, _L().mb_upper_bound)
+
+
 def merge(exec: Executor, left, right, less=O.Less) -> DeviceVec:
     """vector::merge (massively/src/api/algorithm/merge.rs:109)."""
     _check_owner(exec, left, right)

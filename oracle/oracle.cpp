@@ -283,6 +283,26 @@ template <class T> int merge_src_t(const void* l, uint64_t nl, const void* r, ui
   return 0;
 }
 
+// lower_bound / upper_bound: vector.rs:404-426 -- per value, the partition
+// point of the sorted source: first index whose candidate is not less than
+// the value (lower), or that the value is less than (upper).
+template <class T> int bounds_t(const void* src, uint64_t n, const void* vals, uint64_t m,
+                                int less, int upper, uint32_t* out) {
+  const T* a = (const T*)src; const T* v = (const T*)vals;
+  for (uint64_t q = 0; q < m; ++q) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) / 2;
+      const bool in_prefix = upper ? !apply_pred2<T>(less, v[q], a[mid])
+                                   : apply_pred2<T>(less, a[mid], v[q]);
+      if (in_prefix) lo = mid + 1;
+      else hi = mid;
+    }
+    out[q] = (uint32_t)lo;
+  }
+  return 0;
+}
+
 // set_union / set_intersection / set_difference: vector.rs:595-664.
 // mode 0 union, 1 intersection, 2 difference.  Same source encoding.
 template <class T> int64_t set_op_src_t(const void* l, uint64_t nl, const void* r, uint64_t nr,
@@ -517,6 +537,11 @@ int orc_merge_src(int dt, const void* l, uint64_t nl, const void* r, uint64_t nr
 int64_t orc_set_op_src(int dt, const void* l, uint64_t nl, const void* r, uint64_t nr, int less,
                        int mode, uint64_t* src) {
   ORC_DISPATCH(dt, set_op_src_t, l, nl, r, nr, less, mode, src);
+  return -1;
+}
+int orc_bounds(int dt, const void* src, uint64_t n, const void* vals, uint64_t m, int less,
+               int upper, uint32_t* out) {
+  ORC_DISPATCH(dt, bounds_t, src, n, vals, m, less, upper, out);
   return -1;
 }
 int64_t orc_unique(int dt, const void* in, uint64_t n, int eq, void* out) {

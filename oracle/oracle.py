@@ -72,6 +72,7 @@ def _declare(L: C.CDLL) -> None:
         "orc_reduce_by_key_u32": (i64, [vp, vp, u64, i32, u32, vp, vp]),
         "orc_scan_by_key": (i32, [i32, vp, u64, vp, i32, i32, vp, vp]),
         "orc_merge_src": (i32, [i32, vp, u64, vp, u64, i32, vp]),
+        "orc_bounds": (i32, [i32, vp, u64, vp, u64, i32, i32, vp]),
         "orc_set_op_src": (i64, [i32, vp, u64, vp, u64, i32, i32, vp]),
         "orc_unique": (i64, [i32, vp, u64, i32, vp]),
         "orc_seg_scan": (i32, [i32, vp, vp, u64, i32, i32, vp, vp]),
@@ -383,6 +384,24 @@ def merge(left, right, less: str = "less") -> np.ndarray:
     lib().orc_merge_src(_dt(left), _p(left), left.size, _p(right), right.size, PRED2[less],
                         _p(src))
     return _apply_src(src, [left], [right])[0]
+
+
+def lower_bound(source, values, less: str = "less") -> np.ndarray:
+    """vector.rs:404-414: first index whose candidate is not less than each value."""
+    source, values = _c(source), _c(values)
+    out = np.empty(values.size, np.uint32)
+    lib().orc_bounds(_dt(source), _p(source), source.size, _p(values), values.size, PRED2[less],
+                     0, _p(out))
+    return out
+
+
+def upper_bound(source, values, less: str = "less") -> np.ndarray:
+    """vector.rs:416-426: first index whose candidate each value is less than."""
+    source, values = _c(source), _c(values)
+    out = np.empty(values.size, np.uint32)
+    lib().orc_bounds(_dt(source), _p(source), source.size, _p(values), values.size, PRED2[less],
+                     1, _p(out))
+    return out
 
 
 def merge_by_key(lk, lv, rk, rv, less: str = "less"):

@@ -220,6 +220,13 @@ SETS = [
          intersection=np.array([2, 4], U32), difference=np.array([1, 2], U32)),
 ]
 
+BOUNDS = [
+    # api/algorithm/search.rs doctests of lower_bound and upper_bound
+    dict(src="massively/src/api/algorithm/search.rs:75-79, 122-126",
+         source=np.array([1, 3, 5, 7], U32), values=np.array([0, 3, 6, 8], U32),
+         lower=np.array([0, 1, 3, 4], U32), upper=np.array([0, 2, 3, 4], U32)),
+]
+
 UNIQUE = [
     # api/algorithm/ordering.rs:141-144
     dict(src="massively/src/api/algorithm/ordering.rs:141-144",

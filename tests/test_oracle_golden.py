@@ -129,6 +129,20 @@ def test_merge_and_set_known_answers(orc):
         np.testing.assert_array_equal(orc.unique(case["x"]), case["want"])
 
 
+def test_bounds_known_answers(orc):
+    for case in K.BOUNDS:
+        np.testing.assert_array_equal(orc.lower_bound(case["source"], case["values"]),
+                                      case["lower"], err_msg=case["src"])
+        np.testing.assert_array_equal(orc.upper_bound(case["source"], case["values"]),
+                                      case["upper"], err_msg=case["src"])
+    # numpy's searchsorted is the same partition point for `<`
+    rng = np.random.default_rng(3)
+    src = np.sort(rng.integers(0, 50, 1000).astype(np.uint32))
+    vals = rng.integers(0, 60, 500).astype(np.uint32)
+    np.testing.assert_array_equal(orc.lower_bound(src, vals), np.searchsorted(src, vals, "left"))
+    np.testing.assert_array_equal(orc.upper_bound(src, vals), np.searchsorted(src, vals, "right"))
+
+
 def test_seg_known_answers(orc):
     for case in K.SEG:
         if case["kind"] == "reduce":
