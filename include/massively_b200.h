@@ -323,6 +323,16 @@ int mb_exclusive_scan_by_key(mb_executor* exec, const mb_src* keys, int key_eq,
 
 /* --------------------------------------------------------- merge / set ---- */
 
+/* vector::unique (massively/src/api/algorithm/ordering.rs:146) and
+ * vector::unique_by_key (by_key.rs:759): the first item (row of `values`) of
+ * every run of adjacent equal items (keys) under `equal` (MB_EQUAL).  The
+ * kept count is written to count_dev (device) and/or count_host. */
+int mb_unique(mb_executor* exec, const mb_src* input, int equal, mb_col out, uint32_t* count_dev,
+              uint32_t* count_host);
+int mb_unique_by_key(mb_executor* exec, const mb_src* keys, const mb_src* values, int nvals,
+                     int equal, const mb_col* out_values, uint32_t* count_dev,
+                     uint32_t* count_host);
+
 /* vector::lower_bound / vector::upper_bound (massively/src/api/algorithm/
  * search.rs:81-147): for every value, the partition point of the sorted
  * `source` under `less` -- the first index whose element is not less than the

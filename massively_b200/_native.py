@@ -85,6 +85,8 @@ def _declare(L: C.CDLL) -> None:
         "mb_exclusive_scan_by_key": (i32, [vp, src, i32, src, i32, vp, col]),
         "mb_merge": (i32, [vp, src, src, i32, col]),
         "mb_lower_bound": (i32, [vp, src, src, i32, col]),
+        "mb_unique": (i32, [vp, src, i32, col, pu32, pu32]),
+        "mb_unique_by_key": (i32, [vp, src, src, i32, i32, pcol, pu32, pu32]),
         "mb_upper_bound": (i32, [vp, src, src, i32, col]),
         "mb_merge_by_key": (i32, [vp, src, src, src, src, i32, i32, col, pcol]),
         "mb_set_union": (i32, [vp, src, src, i32, col, pu32, pu32]),

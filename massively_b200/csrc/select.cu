@@ -362,9 +362,78 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
 }  // namespace
 }  // namespace mb
 
+namespace mb {
+namespace {
+
+// Run heads of adjacent-equal items: flags[i] = 1 when i == 0 or item i
+// differs from item i-1 (floats compare as values, so NaN differs from
+// itself and -0 equals +0, as massively's Equal does).
+__global__ void __launch_bounds__(kThreads)
+    run_head_flags_kernel(Src keys, uint64_t n, uint32_t* __restrict__ flags) {
+  for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * kThreads) {
+    uint32_t h = 1;
+    if (i > 0) {
+      const uint64_t a = src_load_bits(keys, i - 1), b = src_load_bits(keys, i);
+      if (keys.vtype == MB_F32) h = __uint_as_float((uint32_t)a) != __uint_as_float((uint32_t)b);
+      else if (keys.vtype == MB_F64)
+        h = __longlong_as_double((long long)a) != __longlong_as_double((long long)b);
+      else h = a != b;
+    }
+    flags[i] = h;
+  }
+}
+
+// unique / unique_by_key: the first row of every run of equal keys, kept by
+// the compaction kernel with the run-head flags as its stencil.
+int unique_entry(mb_executor* ex, const mb_src* keys, const mb_src* values, int nvals, int equal,
+                 const mb_col* out, uint32_t* count_dev, uint32_t* count_host) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, keys, "keys"));
+  if (equal != MB_EQUAL) return set_error(MB_ERR_LAUNCH, "unique takes EQUAL");
+  const uint64_t n = keys->len;
+  MB_TRY(check_len_u32(n));
+  Scratch flags;
+  MB_TRY(flags.alloc(ex, std::max<uint64_t>(n, 1) * 4));
+  if (n) {
+    const uint64_t blocks = std::min<uint64_t>((n + kThreads - 1) / kThreads, 148ull * 16);
+    run_head_flags_kernel<<<(unsigned)blocks, kThreads, 0, ex->stream>>>(to_src(*keys), n,
+                                                                         flags.as<uint32_t>());
+    MB_CUDA(cudaGetLastError());
+  }
+  mb_src st{};
+  st.kind = MB_SRC_COLUMN;
+  st.dtype = st.vtype = MB_U32;
+  st.map = MB_UN_IDENTITY;
+  st.data = flags.ptr;
+  st.len = n;
+  st.owner = keys->owner;
+  st.len_dev = keys->len_dev;
+  return select_entry(ex, values, nvals, &st, out, count_dev, count_host, kCopy, nullptr);
+}
+
+}  // namespace
+}  // namespace mb
+
 using namespace mb;
 
 extern "C" {
+
+int mb_unique(mb_executor* ex, const mb_src* input, int equal, mb_col out, uint32_t* count_dev,
+              uint32_t* count_host) {
+  return unique_entry(ex, input, input, 1, equal, &out, count_dev, count_host);
+}
+
+int mb_unique_by_key(mb_executor* ex, const mb_src* keys, const mb_src* values, int nvals,
+                     int equal, const mb_col* out_values, uint32_t* count_dev,
+                     uint32_t* count_host) {
+  if (values && keys && nvals >= 1)
+    for (int c = 0; c < nvals; ++c)
+      if (values[c].len != keys->len)
+        return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", keys->len,
+                         values[c].len);
+  return unique_entry(ex, keys, values, nvals, equal, out_values, count_dev, count_host);
+}
 
 int mb_copy_where(mb_executor* ex, const mb_src* in, int ncols, const mb_src* stencil,
                   const mb_col* out, uint32_t* count_dev, uint32_t* count_host) {

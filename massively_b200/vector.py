@@ -476,6 +476,37 @@ def exclusive_scan_by_key(exec: Executor, keys, values, equal, init, op):
 
 # ---------------------------------------------------------- merge / set --
 
+def unique(exec: Executor, input, equal=O.Equal) -> DeviceVec:
+    """vector::unique (massively/src/api/algorithm/ordering.rs:146): the
+    first item of every run of equal items; the count stays on the device."""
+    _check_owner(exec, input)
+    n = _len(input)
+    keep = []
+    s = lower(exec, input, keep)
+    cnt = _count_buffer(exec)
+    out = exec.alloc(_dtype(input), n).with_len_dev(cnt)
+    check(_L().mb_unique(exec.handle, C.byref(s), O.pred2(equal).id, out.to_col(), _p32(cnt),
+                         None))
+    return out
+
+
+def unique_by_key(exec: Executor, keys, values, equal=O.Equal):
+    """vector::unique_by_key (by_key.rs:759): the values of the first row of
+    every run of equal keys."""
+    _check_owner(exec, keys, values)
+    n, m = _len(keys), _len(values)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    ks = lower(exec, keys, keep)
+    vs, nv = _srcs(exec, values, keep)
+    cnt = _count_buffer(exec)
+    outs = _out_like(exec, values, n, cnt)
+    check(_L().mb_unique_by_key(exec.handle, C.byref(ks), vs, nv, O.pred2(equal).id,
+                                _cols(outs), _p32(cnt), None))
+    return _wrap(values, outs)
+
+
 def _bounds(exec, source, values, less, fn):
     _check_owner(exec, source, values)
     keep = []

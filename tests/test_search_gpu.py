@@ -74,3 +74,34 @@ def test_lazy_values_and_errors(ex):
                                                                                   dtype=np.uint32)))
     with pytest.raises(mb.Launch):
         vector.lower_bound(ex, ds, ex.to_device(np.zeros(3, np.float32)))
+
+
+def test_unique_known_answers(ex):
+    from massively_b200 import vector
+    for case in K.UNIQUE:
+        got = vector.unique(ex, ex.to_device(case["x"]))
+        np.testing.assert_array_equal(ex.to_host(got), case["want"], err_msg=case["src"])
+    # by_key.rs doctest of unique_by_key
+    k = ex.to_device(np.array([1, 1, 2, 2, 3], np.uint32))
+    v = ex.to_device(np.array([10, 11, 20, 21, 30], np.uint32))
+    np.testing.assert_array_equal(ex.to_host(vector.unique_by_key(ex, k, v)), [10, 20, 30])
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 8191, 8192, 8193, 300_001])
+@pytest.mark.parametrize("dtype", [np.uint32, np.int64, np.float32, np.uint16])
+def test_unique_and_by_key(ex, n, dtype):
+    from massively_b200 import iter as I, vector
+    rng = np.random.default_rng(n + 1)
+    x = np.sort(rng.integers(0, max(1, n // 3), n)).astype(dtype)
+    if np.dtype(dtype).kind == "f" and n > 4:
+        x[1] = np.nan
+        x[2] = np.nan
+        x[3] = -0.0
+        x[4] = 0.0
+    np.testing.assert_array_equal(ex.to_host(vector.unique(ex, ex.to_device(x))), orc.unique(x))
+    heads = np.concatenate([[True], x[1:] != x[:-1]]) if n else np.zeros(0, bool)
+    vals = np.arange(n, dtype=np.uint32)
+    got = vector.unique_by_key(ex, ex.to_device(x), I.Zip(ex.to_device(vals), ex.to_device(x)))
+    a, b = got.cols
+    np.testing.assert_array_equal(ex.to_host(a), vals[heads])
+    np.testing.assert_array_equal(ex.to_host(b), x[heads])
