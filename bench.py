@@ -505,7 +505,8 @@ class SimpleWorkload(Workload):
     """A one-call step over resident inputs, reported in GB/s of its byte
     model: reduce (n * 4), merge of two sorted lists ((l + r) * 4 * 2),
     gather through a random permutation (n * 12: indices, the values they
-    pick, the output)."""
+    pick, the output), find_if with no passing item (a full scan, n * 4) and
+    minmax_element over f32 normals (n * 4)."""
 
     kernel = "single call"
 
@@ -514,10 +515,12 @@ class SimpleWorkload(Workload):
         lg = int(np.log2(n))
         self.name = {"reduce": f"reduce_add_u32_2^{lg}", "merge": f"merge_u32_2x2^{lg - 1}",
                      "gather": f"gather_u32_2^{lg}",
-                     "lower_bound": f"lower_bound_u32_2^{lg}_in_2^24"}[kind]
+                     "lower_bound": f"lower_bound_u32_2^{lg}_in_2^24",
+                     "find_if": f"find_if_u32_2^{lg}_no_hit",
+                     "minmax": f"minmax_element_f32_2^{lg}"}[kind]
         self.metric = f"{kind} GB/s"
         self.unit = "GB/s"
-        self.dtype = "u32"
+        self.dtype = "f32" if kind == "minmax" else "u32"
 
     def setup(self, ex):
         from massively_b200 import lazy, vector
@@ -530,6 +533,12 @@ class SimpleWorkload(Workload):
         elif self.kind == "lower_bound":
             self.src = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 13, 1 << 24))
             self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 14, self.n)
+        elif self.kind == "find_if":
+            self.x = device_uniform_u32(ex, 1, 0xFFFFFFFF, 15, self.n)  # no zero: no hit
+            self.res = ex.alloc(np.uint32, 2)
+        elif self.kind == "minmax":
+            self.x = ex.to_device(host_normal_f32(ex, 16, self.n))
+            self.res = ex.alloc(np.uint32, 2)
         else:
             self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 11, self.n)
             r = device_uniform_u32(ex, 0, 0xFFFFFFFF, 12, self.n)
@@ -545,6 +554,10 @@ class SimpleWorkload(Workload):
             self.out = vector.merge(ex, self.a, self.b)
         elif self.kind == "lower_bound":
             self.out = vector.lower_bound(ex, self.src, self.x)
+        elif self.kind == "find_if":
+            vector.find_if(ex, self.x, "is_false", out=self.res)
+        elif self.kind == "minmax":
+            vector.minmax_element(ex, self.x, out=self.res)
         else:
             self.out = vector.gather(ex, self.x, self.idx)
 
@@ -554,7 +567,8 @@ class SimpleWorkload(Workload):
     def alg_bytes(self):
         # lower_bound: each query's value in and index out (the 64 MB source
         # stays in L2 after the first probes)
-        return {"reduce": 4.0, "merge": 8.0, "gather": 12.0, "lower_bound": 8.0}[self.kind] * self.n
+        return {"reduce": 4.0, "merge": 8.0, "gather": 12.0, "lower_bound": 8.0, "find_if": 4.0,
+                "minmax": 4.0}[self.kind] * self.n
 
     def value_from_ms(self, ms, n_gpus):
         return self.alg_bytes() * n_gpus / (ms * 1e-3) / 1e9
@@ -583,10 +597,13 @@ WORKLOADS = {
     "merge_u32": lambda: SimpleWorkload("merge", _n(28)),
     "gather_u32": lambda: SimpleWorkload("gather", _n(28)),
     "lower_bound_u32": lambda: SimpleWorkload("lower_bound", _n(26)),
+    "find_if_u32": lambda: SimpleWorkload("find_if", _n(28)),
+    "minmax_element_f32": lambda: SimpleWorkload("minmax", _n(28)),
 }
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64",
              "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by", "reduce_u32",
-             "merge_u32", "gather_u32", "lower_bound_u32"]
+             "merge_u32", "gather_u32", "lower_bound_u32", "find_if_u32",
+             "minmax_element_f32"]
 
 
 # -------------------------------------------------------------- helpers --

@@ -343,6 +343,62 @@ int mb_lower_bound(mb_executor* exec, const mb_src* source, const mb_src* values
 int mb_upper_bound(mb_executor* exec, const mb_src* source, const mb_src* values, int less,
                    mb_col out);
 
+/* ------------------------------------- first-index searches and extrema ---- */
+
+/* Each writes one u32 to result_dev (device, stream-ordered: usable inside a
+ * graph capture) and / or result_host (synchronises).  An index result is
+ * MB_NONE (MIndex::MAX) for massively's None; a flag result is 0 or 1.
+ * Predicates `pred` are the mb_unary IS_* ids (IS_EVEN / IS_ODD on integer
+ * items only); `equal` is MB_EQUAL; `less` is LESS, GREATER or TOTAL_LESS.
+ *
+ * mb_find_if         vector::find_if (predicate.rs:218): first passing item.
+ * mb_is_partitioned  vector::is_partitioned (predicate.rs:225-260): flag, no
+ *                    passing item after a failing one.
+ * mb_adjacent_find   vector::adjacent_find (ordering.rs:107): first i with
+ *                    x[i] == x[i+1].
+ * mb_is_sorted_until vector::is_sorted_until (ordering.rs:213): first i with
+ *                    less(x[i], x[i-1]), else the length; is_sorted
+ *                    (ordering.rs:256) is "result == length".
+ * mb_find_first_of   vector::find_first_of (search.rs:33): first source item
+ *                    equal to any needle.
+ * mb_mismatch        vector::mismatch (search.rs:231): first i below the
+ *                    shorter length with left[i] != right[i]; else the
+ *                    shorter length when the lengths differ, else None.
+ * mb_equal           vector::equal (search.rs:175): flag.
+ * mb_lexicographical_compare  vector::lexicographical_compare
+ *                    (search.rs:289): flag, left before right. */
+#define MB_NONE 0xFFFFFFFFu
+int mb_find_if(mb_executor* exec, const mb_src* input, int pred, uint32_t* result_dev,
+               uint32_t* result_host);
+int mb_is_partitioned(mb_executor* exec, const mb_src* input, int pred, uint32_t* result_dev,
+                      uint32_t* result_host);
+int mb_adjacent_find(mb_executor* exec, const mb_src* input, int equal, uint32_t* result_dev,
+                     uint32_t* result_host);
+int mb_is_sorted_until(mb_executor* exec, const mb_src* input, int less, uint32_t* result_dev,
+                       uint32_t* result_host);
+int mb_find_first_of(mb_executor* exec, const mb_src* source, const mb_src* needles, int equal,
+                     uint32_t* result_dev, uint32_t* result_host);
+int mb_mismatch(mb_executor* exec, const mb_src* left, const mb_src* right, int equal,
+                uint32_t* result_dev, uint32_t* result_host);
+int mb_equal(mb_executor* exec, const mb_src* left, const mb_src* right, int equal,
+             uint32_t* result_dev, uint32_t* result_host);
+int mb_lexicographical_compare(mb_executor* exec, const mb_src* left, const mb_src* right,
+                               int less, uint32_t* result_dev, uint32_t* result_host);
+
+/* vector::min_element / max_element / minmax_element (ordering.rs:300-380,
+ * core massively/src/core/arg_reduce.rs): the first minimum, the first
+ * maximum, and (minmax: two u32, minimum then maximum) the LAST minimum with
+ * the first maximum, as massively's sequential definition gives them; MB_NONE
+ * for an empty input.  Under LESS / GREATER a float NaN behaves as in that
+ * sequential scan (a NaN at index 0 is the first minimum and maximum; minmax's
+ * minimum restarts after the last NaN). */
+int mb_min_element(mb_executor* exec, const mb_src* input, int less, uint32_t* result_dev,
+                   uint32_t* result_host);
+int mb_max_element(mb_executor* exec, const mb_src* input, int less, uint32_t* result_dev,
+                   uint32_t* result_host);
+int mb_minmax_element(mb_executor* exec, const mb_src* input, int less, uint32_t* result_dev,
+                      uint32_t* result_host);
+
 /* vector::merge (massively/src/api/algorithm/merge.rs:109; core
  * massively/src/core/merge.rs:24-1230): stable merge, left first on ties. */
 int mb_merge(mb_executor* exec, const mb_src* left, const mb_src* right, int less, mb_col out);
@@ -446,7 +502,8 @@ enum {
   MB_KF_RADIX_ONESWEEP = 0,  /* one onesweep digit pass */
   MB_KF_RADIX_HISTOGRAM = 1, /* the all-digit histogram */
   MB_KF_SCAN = 2,            /* inclusive / exclusive scan */
-  MB_KF_SELECT = 3           /* copy_where / remove_where / partition */
+  MB_KF_SELECT = 3,          /* copy_where / remove_where / partition */
+  MB_KF_SEARCH = 4           /* first-index searches and extrema (predicate.cu) */
 };
 int mb_kernel_timing(mb_executor* exec, int enable);
 int mb_kernel_timing_read(mb_executor* exec, int family, uint64_t* launches, double* total_ms);

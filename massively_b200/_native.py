@@ -19,7 +19,7 @@ OK, LENGTH_MISMATCH, OUTPUT_TOO_SHORT, LENGTH_TOO_LARGE, INVALID_SEGMENTATION, \
     UNBOUND_COLUMN, FOREIGN_EXECUTOR, LAUNCH = range(8)
 SRC_COLUMN, SRC_CONSTANT, SRC_COUNTING, SRC_STRIDE, SRC_PERMUTE, SRC_REVERSE, \
     SRC_REPEAT_EACH, SRC_TILE, SRC_ADJACENT = range(9)
-KF_RADIX_ONESWEEP, KF_RADIX_HISTOGRAM, KF_SCAN, KF_SELECT = range(4)
+KF_RADIX_ONESWEEP, KF_RADIX_HISTOGRAM, KF_SCAN, KF_SELECT, KF_SEARCH = range(5)
 
 
 class mb_src(C.Structure):
@@ -86,6 +86,17 @@ def _declare(L: C.CDLL) -> None:
         "mb_merge": (i32, [vp, src, src, i32, col]),
         "mb_lower_bound": (i32, [vp, src, src, i32, col]),
         "mb_unique": (i32, [vp, src, i32, col, pu32, pu32]),
+        "mb_find_if": (i32, [vp, src, i32, pu32, pu32]),
+        "mb_is_partitioned": (i32, [vp, src, i32, pu32, pu32]),
+        "mb_adjacent_find": (i32, [vp, src, i32, pu32, pu32]),
+        "mb_is_sorted_until": (i32, [vp, src, i32, pu32, pu32]),
+        "mb_find_first_of": (i32, [vp, src, src, i32, pu32, pu32]),
+        "mb_mismatch": (i32, [vp, src, src, i32, pu32, pu32]),
+        "mb_equal": (i32, [vp, src, src, i32, pu32, pu32]),
+        "mb_lexicographical_compare": (i32, [vp, src, src, i32, pu32, pu32]),
+        "mb_min_element": (i32, [vp, src, i32, pu32, pu32]),
+        "mb_max_element": (i32, [vp, src, i32, pu32, pu32]),
+        "mb_minmax_element": (i32, [vp, src, i32, pu32, pu32]),
         "mb_unique_by_key": (i32, [vp, src, src, i32, i32, pcol, pu32, pu32]),
         "mb_upper_bound": (i32, [vp, src, src, i32, col]),
         "mb_merge_by_key": (i32, [vp, src, src, src, src, i32, i32, col, pcol]),

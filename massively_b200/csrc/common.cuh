@@ -480,7 +480,13 @@ template <class K>
 __device__ __forceinline__ typename UnsignedOf<K>::type radix_enc(K k) {
   using U = typename UnsignedOf<K>::type;
   U raw;
-  memcpy(&raw, &k, sizeof(U));
+  if constexpr (std::is_same<K, double>::value) {
+    raw = (U)__double_as_longlong(k);  // the bit pattern, NaN payloads included
+  } else if constexpr (std::is_same<K, float>::value) {
+    raw = (U)__float_as_uint(k);
+  } else {
+    memcpy(&raw, &k, sizeof(U));
+  }
   constexpr U sign = (U)1 << (sizeof(U) * 8 - 1);
   if constexpr (std::is_floating_point<K>::value) {
     return (raw & sign) ? (U)~raw : (U)(raw ^ sign);

@@ -33,10 +33,16 @@ namespace mb {
 constexpr uint32_t kFlagNone = 0, kFlagAgg = 1, kFlagIncl = 2;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
+// Floating values are cast with the bit-reinterpreting intrinsics: they keep
+// NaN bit patterns exactly.
 template <class T>
 __device__ __forceinline__ uint64_t to_bits64(T v) {
   static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte value");
-  if constexpr (sizeof(T) == 4) {
+  if constexpr (std::is_same<T, double>::value) {
+    return (uint64_t)__double_as_longlong(v);
+  } else if constexpr (std::is_same<T, float>::value) {
+    return __float_as_uint(v);
+  } else if constexpr (sizeof(T) == 4) {
     uint32_t b;
     memcpy(&b, &v, 4);
     return b;
@@ -49,7 +55,11 @@ __device__ __forceinline__ uint64_t to_bits64(T v) {
 template <class T>
 __device__ __forceinline__ T from_bits64(uint64_t b) {
   T v;
-  if constexpr (sizeof(T) == 4) {
+  if constexpr (std::is_same<T, double>::value) {
+    v = __longlong_as_double((long long)b);
+  } else if constexpr (std::is_same<T, float>::value) {
+    v = __uint_as_float((uint32_t)b);
+  } else if constexpr (sizeof(T) == 4) {
     uint32_t w = (uint32_t)b;
     memcpy(&v, &w, 4);
   } else {

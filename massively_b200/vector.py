@@ -18,7 +18,7 @@ import torch
 from . import _native as N
 from . import op as O
 from .iter import Zip
-from .lazy import View, lower
+from .lazy import Map, View, lower
 from .runtime import (ID_TO_NP, DeviceVec, Executor, ForeignExecutor, LengthMismatch,
                       LengthTooLarge, MINDEX_MAX, check, scalar_buffer)
 
@@ -530,6 +530,147 @@ def upper_bound(exec: Executor, source, values, less=O.Less) -> DeviceVec:
     """vector::upper_bound (search.rs:128): per value, the first index of
     the sorted source greater than it."""
     return _bounds(exec, source, values, less, _L().mb_upper_bound)
+
+
+# ------------------------------------------- predicates and first index --
+#
+# Each query's result is one u32 on the device: an index (MINDEX_MAX for
+# massively's None) or a 0 / 1 flag.  By default it is read back (as
+# massively does: "this operation synchronizes to resolve the optional index
+# on the host"); with `out` (a u32 DeviceVec, two items for minmax_element)
+# it stays on the device, stream-ordered, so the call needs no host
+# synchronisation and may sit inside a graph capture.
+
+def _query(exec, fn, inputs, op, out, count=1):
+    _check_owner(exec, *inputs)
+    keep = []
+    srcs = []
+    for x in inputs:
+        _len(x)
+        srcs.append(C.byref(lower(exec, x, keep)))
+    if out is not None:
+        if out.dtype != np.uint32 or len(out) < count:
+            raise ValueError(f"out must be a u32 DeviceVec of at least {count} item(s)")
+        check(fn(exec.handle, *srcs, op, _p32(out.tensor), None))
+        return None
+    res = (C.c_uint32 * 2)()
+    check(fn(exec.handle, *srcs, op, None, res))
+    return list(res)[:count]
+
+
+def _opt(r):
+    return None if r is None or r == MINDEX_MAX else int(r)
+
+
+def count_if(exec: Executor, input, pred) -> int:
+    """vector::count_if (massively/src/api/algorithm/predicate.rs:63-90): the
+    number of items the predicate passes -- a sum reduction of the
+    predicate's 0 / 1 flags (core/predicate.rs:195-202)."""
+    _check_owner(exec, input)
+    _len(input)
+    return int(reduce(exec, Map(input, O.unary(pred)), 0, O.Add))
+
+
+def all_of(exec: Executor, input, pred) -> bool:
+    """vector::all_of (predicate.rs:93-122): count_if == length."""
+    return count_if(exec, input, pred) == _len(input)
+
+
+def any_of(exec: Executor, input, pred) -> bool:
+    """vector::any_of (predicate.rs:125-154); answered by the first-index
+    search, which stops at the first passing item."""
+    return find_if(exec, input, pred) is not None
+
+
+def none_of(exec: Executor, input, pred) -> bool:
+    """vector::none_of (predicate.rs:157-186)."""
+    return find_if(exec, input, pred) is None
+
+
+def find_if(exec: Executor, input, pred, out: DeviceVec | None = None):
+    """vector::find_if (predicate.rs:218): the first passing position, or
+    None."""
+    r = _query(exec, _L().mb_find_if, [input], O.unary(pred).id, out)
+    return None if r is None else _opt(r[0])
+
+
+def is_partitioned(exec: Executor, input, pred, out: DeviceVec | None = None):
+    """vector::is_partitioned (predicate.rs:232-260): no passing item after
+    a failing one."""
+    r = _query(exec, _L().mb_is_partitioned, [input], O.unary(pred).id, out)
+    return None if r is None else bool(r[0])
+
+
+def adjacent_find(exec: Executor, input, equal=O.Equal, out: DeviceVec | None = None):
+    """vector::adjacent_find (massively/src/api/algorithm/ordering.rs:107):
+    the first i with equal(x[i], x[i+1]), or None."""
+    r = _query(exec, _L().mb_adjacent_find, [input], O.pred2(equal).id, out)
+    return None if r is None else _opt(r[0])
+
+
+def is_sorted_until(exec: Executor, input, less=O.Less, out: DeviceVec | None = None):
+    """vector::is_sorted_until (ordering.rs:213): the first i with
+    less(x[i], x[i-1]), else the length."""
+    r = _query(exec, _L().mb_is_sorted_until, [input], O.pred2(less).id, out)
+    return None if r is None else int(r[0])
+
+
+def is_sorted(exec: Executor, input, less=O.Less) -> bool:
+    """vector::is_sorted (ordering.rs:256)."""
+    return is_sorted_until(exec, input, less) == _len(input)
+
+
+def find_first_of(exec: Executor, source, needles, equal=O.Equal,
+                  out: DeviceVec | None = None):
+    """vector::find_first_of (massively/src/api/algorithm/search.rs:33): the
+    first source item equal to any needle, or None."""
+    r = _query(exec, _L().mb_find_first_of, [source, needles], O.pred2(equal).id, out)
+    return None if r is None else _opt(r[0])
+
+
+def equal(exec: Executor, left, right, eq=O.Equal, out: DeviceVec | None = None):
+    """vector::equal (search.rs:175): equal lengths and every pair equal."""
+    r = _query(exec, _L().mb_equal, [left, right], O.pred2(eq).id, out)
+    return None if r is None else bool(r[0])
+
+
+def mismatch(exec: Executor, left, right, eq=O.Equal, out: DeviceVec | None = None):
+    """vector::mismatch (search.rs:231): the first differing position; past
+    an equal common prefix, the shorter length if the lengths differ, else
+    None."""
+    r = _query(exec, _L().mb_mismatch, [left, right], O.pred2(eq).id, out)
+    return None if r is None else _opt(r[0])
+
+
+def lexicographical_compare(exec: Executor, left, right, less=O.Less,
+                            out: DeviceVec | None = None):
+    """vector::lexicographical_compare (search.rs:289): left orders before
+    right."""
+    r = _query(exec, _L().mb_lexicographical_compare, [left, right], O.pred2(less).id, out)
+    return None if r is None else bool(r[0])
+
+
+def min_element(exec: Executor, input, less=O.Less, out: DeviceVec | None = None):
+    """vector::min_element (ordering.rs:300-327): the first minimum's index,
+    or None."""
+    r = _query(exec, _L().mb_min_element, [input], O.pred2(less).id, out)
+    return None if r is None else _opt(r[0])
+
+
+def max_element(exec: Executor, input, less=O.Less, out: DeviceVec | None = None):
+    """vector::max_element (ordering.rs:328-360): the first maximum's index,
+    or None."""
+    r = _query(exec, _L().mb_max_element, [input], O.pred2(less).id, out)
+    return None if r is None else _opt(r[0])
+
+
+def minmax_element(exec: Executor, input, less=O.Less, out: DeviceVec | None = None):
+    """vector::minmax_element (ordering.rs:361-412): (last minimum, first
+    maximum) as massively's sequential definition keeps them, or None."""
+    r = _query(exec, _L().mb_minmax_element, [input], O.pred2(less).id, out, count=2)
+    if r is None:
+        return None
+    return None if r[0] == MINDEX_MAX else (int(r[0]), int(r[1]))
 
 
 def merge(exec: Executor, left, right, less=O.Less) -> DeviceVec:

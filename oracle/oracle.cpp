@@ -380,6 +380,92 @@ inline uint32_t pcg_hash32(uint32_t input) {
   return (word >> 22) ^ word;
 }
 
+// First-index searches and flags (vector.rs:176-218, 317-378), one entry
+// for all of them; the result uses the C ABI's encoding: an index, MB_NONE
+// for None, or a 0 / 1 flag.
+//   0 find_if           vector.rs:212   position of the first passing item
+//   1 is_partitioned    core/predicate.rs:111-127: no passing item after a
+//                       failing one (flag)
+//   2 adjacent_find     vector.rs:344   first i with eq(x[i], x[i+1])
+//   3 is_sorted_until   vector.rs:367   first i >= 1 with less(x[i], x[i-1]),
+//                                       else len
+//   4 mismatch          vector.rs:330
+//   5 equal             vector.rs:317   (flag)
+//   6 lexicographical_compare  vector.rs:388 (flag)
+//   7 find_first_of     vector.rs:354
+template <class T> int64_t find_t(int kind, const void* av, uint64_t na, const void* bv,
+                                  uint64_t nb, int op) {
+  const T* a = (const T*)av; const T* b = (const T*)bv;
+  const int64_t none = (int64_t)MB_NONE;
+  switch (kind) {
+    case 0:
+      for (uint64_t i = 0; i < na; ++i) if (apply_flag<T>(op, a[i])) return (int64_t)i;
+      return none;
+    case 1: {
+      uint64_t i = 0;
+      while (i < na && apply_flag<T>(op, a[i])) ++i;
+      while (i < na && !apply_flag<T>(op, a[i])) ++i;
+      return i == na ? 1 : 0;
+    }
+    case 2:
+      for (uint64_t i = 0; i + 1 < na; ++i) if (apply_pred2<T>(MB_EQUAL, a[i], a[i + 1])) return (int64_t)i;
+      return none;
+    case 3:
+      for (uint64_t i = 1; i < na; ++i) if (apply_pred2<T>(op, a[i], a[i - 1])) return (int64_t)i;
+      return (int64_t)na;
+    case 4: {
+      const uint64_t n = std::min(na, nb);
+      for (uint64_t i = 0; i < n; ++i) if (!apply_pred2<T>(MB_EQUAL, a[i], b[i])) return (int64_t)i;
+      return na != nb ? (int64_t)n : none;
+    }
+    case 5: {
+      if (na != nb) return 0;
+      for (uint64_t i = 0; i < na; ++i) if (!apply_pred2<T>(MB_EQUAL, a[i], b[i])) return 0;
+      return 1;
+    }
+    case 6: {
+      const uint64_t n = std::min(na, nb);
+      for (uint64_t i = 0; i < n; ++i) {
+        if (apply_pred2<T>(op, a[i], b[i])) return 1;
+        if (apply_pred2<T>(op, b[i], a[i])) return 0;
+      }
+      return na < nb ? 1 : 0;
+    }
+    case 7:
+      for (uint64_t i = 0; i < na; ++i)
+        for (uint64_t k = 0; k < nb; ++k)
+          if (apply_pred2<T>(MB_EQUAL, a[i], b[k])) return (int64_t)i;
+      return none;
+    default: return -1;
+  }
+}
+
+// min_element / max_element / minmax_element: vector.rs:428-481, the
+// sequential scans themselves (first minimum; first maximum; minmax moves its
+// minimum on !less(x[min], x[i]) -- the last minimum -- and its maximum on
+// less(x[max], x[i])).  out[0] (and out[1] for minmax) = index or MB_NONE.
+template <class T> int arg_t(int kind, const void* in, uint64_t n, int less, uint32_t* out) {
+  const T* x = (const T*)in;
+  if (n == 0) {
+    out[0] = MB_NONE;
+    if (kind == 2) out[1] = MB_NONE;
+    return 0;
+  }
+  uint64_t mn = 0, mx = 0;
+  for (uint64_t i = 1; i < n; ++i) {
+    switch (kind) {
+      case 0: if (apply_pred2<T>(less, x[i], x[mn])) mn = i; break;
+      case 1: if (apply_pred2<T>(less, x[mx], x[i])) mx = i; break;
+      default:
+        if (!apply_pred2<T>(less, x[mn], x[i])) mn = i;
+        if (apply_pred2<T>(less, x[mx], x[i])) mx = i;
+    }
+  }
+  out[0] = (uint32_t)(kind == 1 ? mx : mn);
+  if (kind == 2) out[1] = (uint32_t)mx;
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -542,6 +628,15 @@ int64_t orc_set_op_src(int dt, const void* l, uint64_t nl, const void* r, uint64
 int orc_bounds(int dt, const void* src, uint64_t n, const void* vals, uint64_t m, int less,
                int upper, uint32_t* out) {
   ORC_DISPATCH(dt, bounds_t, src, n, vals, m, less, upper, out);
+  return -1;
+}
+int64_t orc_find(int kind, int dt, const void* a, uint64_t na, const void* b, uint64_t nb,
+                 int op) {
+  ORC_DISPATCH(dt, find_t, kind, a, na, b, nb, op);
+  return -1;
+}
+int orc_arg(int kind, int dt, const void* in, uint64_t n, int less, uint32_t* out) {
+  ORC_DISPATCH(dt, arg_t, kind, in, n, less, out);
   return -1;
 }
 int64_t orc_unique(int dt, const void* in, uint64_t n, int eq, void* out) {

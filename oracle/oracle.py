@@ -75,6 +75,8 @@ def _declare(L: C.CDLL) -> None:
         "orc_bounds": (i32, [i32, vp, u64, vp, u64, i32, i32, vp]),
         "orc_set_op_src": (i64, [i32, vp, u64, vp, u64, i32, i32, vp]),
         "orc_unique": (i64, [i32, vp, u64, i32, vp]),
+        "orc_find": (i64, [i32, i32, vp, u64, vp, u64, i32]),
+        "orc_arg": (i32, [i32, i32, vp, u64, i32, vp]),
         "orc_seg_scan": (i32, [i32, vp, vp, u64, i32, i32, vp, vp]),
         "orc_seg_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp]),
         "orc_seg_sort": (i32, [i32, vp, vp, u64, i32, vp]),
@@ -449,6 +451,114 @@ def unique(x, eq: str = "equal") -> np.ndarray:
 
 
 # --------------------------------------------------------------------- seg --
+
+NONE = 0xFFFFFFFF  # MIndex::MAX, massively's None
+
+
+def _find(kind: int, a, b=None, op: int = 0):
+    a = _c(a)
+    b = a if b is None else _c(b)
+    if a.dtype != b.dtype:
+        raise TypeError("element types differ")
+    r = lib().orc_find(kind, _dt(a), _p(a), a.size, _p(b), b.size, op)
+    if r < 0:
+        raise TypeError(a.dtype)
+    return int(r)
+
+
+def _opt(r: int):
+    return None if r == NONE else r
+
+
+def count_if(x, pred: str) -> int:
+    """vector.rs:176-186."""
+    return int(flags(x, pred).sum())
+
+
+def all_of(x, pred: str) -> bool:
+    """vector.rs:188-194."""
+    return bool(flags(x, pred).all())
+
+
+def any_of(x, pred: str) -> bool:
+    """vector.rs:196-202."""
+    return bool(flags(x, pred).any())
+
+
+def none_of(x, pred: str) -> bool:
+    """vector.rs:204-210."""
+    return not any_of(x, pred)
+
+
+def find_if(x, pred: str):
+    """vector.rs:212-218: first passing position, or None."""
+    return _opt(_find(0, x, op=UNARY[pred]))
+
+
+def is_partitioned(x, pred: str) -> bool:
+    """massively/src/core/predicate.rs:111-127, 213-223: no passing item
+    follows a failing one."""
+    return bool(_find(1, x, op=UNARY[pred]))
+
+
+def adjacent_find(x, eq: str = "equal"):
+    """vector.rs:344-352."""
+    return _opt(_find(2, x))
+
+
+def is_sorted_until(x, less: str = "less") -> int:
+    """vector.rs:367-377."""
+    return _find(3, x, op=PRED2[less])
+
+
+def is_sorted(x, less: str = "less") -> bool:
+    """vector.rs:379-386."""
+    return is_sorted_until(x, less) == np.asarray(x).size
+
+
+def mismatch(left, right, eq: str = "equal"):
+    """vector.rs:330-342."""
+    return _opt(_find(4, left, right))
+
+
+def equal(left, right, eq: str = "equal") -> bool:
+    """vector.rs:317-328."""
+    return bool(_find(5, left, right))
+
+
+def lexicographical_compare(left, right, less: str = "less") -> bool:
+    """vector.rs:388-402."""
+    return bool(_find(6, left, right, PRED2[less]))
+
+
+def find_first_of(source, needles, eq: str = "equal"):
+    """vector.rs:354-365."""
+    return _opt(_find(7, source, needles))
+
+
+def _arg(kind: int, x, less: str):
+    x = _c(x)
+    out = np.zeros(2, np.uint32)
+    if lib().orc_arg(kind, _dt(x), _p(x), x.size, PRED2[less], _p(out)) != 0:
+        raise TypeError(x.dtype)
+    return out
+
+
+def min_element(x, less: str = "less"):
+    """vector.rs:428-443: first minimum, or None."""
+    return _opt(int(_arg(0, x, less)[0]))
+
+
+def max_element(x, less: str = "less"):
+    """vector.rs:445-460: first maximum, or None."""
+    return _opt(int(_arg(1, x, less)[0]))
+
+
+def minmax_element(x, less: str = "less"):
+    """vector.rs:462-481: (last minimum, first maximum), or None."""
+    o = _arg(2, x, less)
+    return None if o[0] == NONE else (int(o[0]), int(o[1]))
+
 
 def validate_offsets(offsets):
     """Segmentation::from_offsets rules; value count, or None if invalid."""

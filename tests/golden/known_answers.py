@@ -233,6 +233,59 @@ UNIQUE = [
          x=np.array([1, 1, 2, 2, 3], U32), want=np.array([1, 2, 3], U32)),
 ]
 
+# Predicates, first-index searches and extrema: the doctests of
+# massively/src/api/algorithm/{predicate,ordering,search}.rs and the unit tests
+# of massively/src/core/predicate.rs.  `fn` names the vector:: function; `a`
+# (and `b`) the inputs; `arg` the predicate (mb_unary name) or order; `want`
+# the result (None for massively's None).
+PREDICATES = [
+    dict(src="massively/src/api/algorithm/predicate.rs:87-89", fn="count_if",
+         a=np.array([1, 2, 3, 4], U32), arg="is_even", want=2),
+    dict(src="massively/src/api/algorithm/predicate.rs:117-121", fn="all_of",
+         a=np.array([2, 4, 6], U32), arg="is_even", want=True),
+    dict(src="massively/src/api/algorithm/predicate.rs:149-153", fn="any_of",
+         a=np.array([1, 3, 4], U32), arg="is_even", want=True),
+    dict(src="massively/src/api/algorithm/predicate.rs:181-185", fn="none_of",
+         a=np.array([1, 3, 5], U32), arg="is_even", want=True),
+    dict(src="massively/src/api/algorithm/predicate.rs:210-215", fn="find_if",
+         a=np.array([1, 3, 4, 6], U32), arg="is_even", want=2),
+    dict(src="massively/src/api/algorithm/predicate.rs:256-260", fn="is_partitioned",
+         a=np.array([2, 4, 1, 3], U32), arg="is_even", want=True),
+    dict(src="massively/src/core/predicate.rs:354-361", fn="count_if",
+         a=np.array([7, 0, 3], U32), arg="is_true", want=2),
+    dict(src="massively/src/core/predicate.rs:364-376", fn="is_partitioned",
+         a=np.array([20, 0], U32), arg="is_even", want=True),
+    dict(src="massively/src/core/predicate.rs:424-431", fn="find_if",
+         a=np.array([1, 3, 5, 7], U32), arg="is_negative", want=None),
+    dict(src="massively/tests/vector/api/runtime.rs:97-99", fn="find_if",
+         a=np.array([], U32), arg="is_even", want=None),
+    dict(src="massively/src/api/algorithm/ordering.rs:99-105", fn="adjacent_find",
+         a=np.array([1, 2, 2, 3], U32), arg="equal", want=1),
+    dict(src="massively/src/api/algorithm/ordering.rs:205-210", fn="is_sorted_until",
+         a=np.array([1, 2, 4, 3, 5], U32), arg="less", want=3),
+    dict(src="massively/src/api/algorithm/ordering.rs:249-253", fn="is_sorted",
+         a=np.array([1, 2, 3, 4], U32), arg="less", want=True),
+    dict(src="massively/src/api/algorithm/ordering.rs:315-321", fn="min_element",
+         a=np.array([3, 1, 2, 1], U32), arg="less", want=1),
+    dict(src="massively/src/api/algorithm/ordering.rs:348-354", fn="max_element",
+         a=np.array([3, 1, 3, 2], U32), arg="less", want=0),
+    dict(src="massively/src/api/algorithm/ordering.rs:404-410", fn="minmax_element",
+         a=np.array([3, 1, 4, 2], U32), arg="less", want=(1, 2)),
+    dict(src="massively/src/api/algorithm/search.rs:26-31", fn="find_first_of",
+         a=np.array([1, 2, 3, 4], U32), b=np.array([7, 3], U32), arg="equal", want=2),
+    dict(src="massively/src/api/algorithm/search.rs:167-172", fn="equal",
+         a=np.array([1, 2, 3], U32), b=np.array([1, 2, 3], U32), arg="equal", want=True),
+    dict(src="massively/src/api/algorithm/search.rs:223-229", fn="mismatch",
+         a=np.array([1, 2, 3], U32), b=np.array([1, 4, 3], U32), arg="equal", want=1),
+    dict(src="massively/src/api/algorithm/search.rs:281-286", fn="lexicographical_compare",
+         a=np.array([1, 2, 3], U32), b=np.array([1, 3, 0], U32), arg="less", want=True),
+]
+
+# massively/tests/vector/api/predicate.rs:17-22: count_if over a lazy
+# counting view of four billion items (u32 lengths above i32::MAX).
+COUNT_IF_FOUR_BILLION = dict(src="massively/tests/vector/api/predicate.rs:17-22",
+                             n=4_000_000_000, pred="is_even", want=2_000_000_000)
+
 SEG = [
     # tests/seg/api.rs:288-322: Reduce(Add, 0) over offsets [0,3,5]
     dict(src="massively/tests/seg/api.rs:288-322", kind="reduce", op="add", init=0,

@@ -143,6 +143,49 @@ def test_bounds_known_answers(orc):
     np.testing.assert_array_equal(orc.upper_bound(src, vals), np.searchsorted(src, vals, "right"))
 
 
+def _call_predicate(mod, case):
+    fn = getattr(mod, case["fn"])
+    return fn(case["a"], case["b"], case["arg"]) if "b" in case else fn(case["a"], case["arg"])
+
+
+def test_predicate_known_answers(orc):
+    for case in K.PREDICATES:
+        assert _call_predicate(orc, case) == case["want"], case["src"]
+
+
+def test_predicate_edges(orc):
+    u = np.uint32
+    # mismatch: equal prefix but different lengths -> the shorter length
+    assert orc.mismatch(np.array([1, 2], u), np.array([1, 2, 3], u)) == 2
+    assert orc.mismatch(np.array([1, 2], u), np.array([1, 2], u)) is None
+    assert orc.equal(np.array([1, 2], u), np.array([1, 2, 3], u)) is False
+    assert orc.lexicographical_compare(np.array([1, 2], u), np.array([1, 2, 3], u)) is True
+    assert orc.lexicographical_compare(np.array([1, 2, 3], u), np.array([1, 2], u)) is False
+    assert orc.is_sorted_until(np.array([], u)) == 0
+    assert orc.min_element(np.array([], u)) is None
+    assert orc.minmax_element(np.array([], u)) is None
+    # minmax keeps the LAST minimum and the FIRST maximum
+    assert orc.minmax_element(np.array([2, 1, 5, 1, 5], u)) == (3, 2)
+    assert orc.min_element(np.array([2, 1, 5, 1, 5], u)) == 1
+    assert orc.max_element(np.array([2, 1, 5, 1, 5], u)) == 2
+    # NaN under `<`: at index 0 it is the first minimum / maximum; elsewhere
+    # never taken; minmax's minimum restarts after the last NaN
+    nan = np.float32("nan")
+    f = np.float32
+    assert orc.min_element(np.array([nan, -1, -2], f)) == 0
+    assert orc.max_element(np.array([1, nan, 3], f)) == 2
+    assert orc.minmax_element(np.array([0, -5, nan, 3, 4], f)) == (3, 4)
+    assert orc.minmax_element(np.array([0, -5, nan], f)) == (2, 0)
+    # numpy agrees on NaN-free input
+    rng = np.random.default_rng(11)
+    x = rng.integers(0, 100, 5000).astype(np.int32)
+    assert orc.min_element(x) == int(np.argmin(x))
+    assert orc.max_element(x) == int(np.argmax(x))
+    assert orc.minmax_element(x)[0] == int(np.flatnonzero(x == x.min())[-1])
+    assert orc.find_if(x, "is_negative") is None
+    assert orc.count_if(x, "is_odd") == int((x % 2 == 1).sum())
+
+
 def test_seg_known_answers(orc):
     for case in K.SEG:
         if case["kind"] == "reduce":
