@@ -89,62 +89,181 @@ __device__ __forceinline__ uint32_t ld_word(const uint32_t* p) {
   return *(const volatile uint32_t*)p;
 }
 
-// The tile walk shared by every first-index search.  `hit(i)` tells whether
-// item i < n qualifies.  All exits are block-uniform.
-template <class HIT>
-__device__ __forceinline__ void first_hit_tiles(uint64_t n, uint32_t* best, HIT hit) {
-  for (uint64_t base = blockIdx.x * (uint64_t)kTile; base < n;
-       base += (uint64_t)gridDim.x * kTile) {
-    if (__syncthreads_or(base >= (uint64_t)ld_word(best))) return;
-    bool h[kItems];
+// Tile geometry.  On a plain, 16-byte-aligned column a thread reads VECS
+// 16-byte vectors per tile (vector v of thread t covers items
+// base + (v * kThreads + t) * VEC ...  + VEC - 1, so a warp's loads are
+// contiguous); other views and the last, partial tile are read item by item
+// (item j of thread t: base + j * kThreads + t).  Either way a thread's items
+// of a tile come in increasing index order.
+template <class T>
+struct Geo {
+  static constexpr int VEC = 16 / (int)sizeof(T);
+  static constexpr int VECS = 4;
+  static constexpr int ITEMS = VEC * VECS;       // per thread and tile
+  static constexpr int TILE = kThreads * ITEMS;  // 4096 4-byte or 2048 8-byte items
+};
+
+template <class T>
+__device__ __forceinline__ uint64_t vec_index(uint64_t base, int v, int e) {
+  return base + ((uint64_t)v * kThreads + threadIdx.x) * Geo<T>::VEC + e;
+}
+
+template <class T>
+__device__ __forceinline__ void load_vecs(const T* __restrict__ p, uint64_t base,
+                                          T (&x)[Geo<T>::VECS][Geo<T>::VEC]) {
 #pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-      const uint64_t i = base + (uint64_t)j * kThreads + threadIdx.x;
-      h[j] = i < n && hit(i);
-    }
-    uint32_t first = kNone;
-#pragma unroll
-    for (int j = kItems - 1; j >= 0; --j)
-      if (h[j]) first = (uint32_t)(base + (uint64_t)j * kThreads + threadIdx.x);
-    if (first != kNone) atomicMin(best, first);
-    if (__syncthreads_or(first != kNone)) return;
+  for (int v = 0; v < Geo<T>::VECS; ++v) {
+    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(p + base) + v * kThreads + threadIdx.x);
+    memcpy(x[v], &u, 16);
   }
 }
+
+template <class T>
+__device__ __forceinline__ T shfl_t(T v, int src_lane) {
+  if constexpr (sizeof(T) == 8)
+    return from_bits64<T>(__shfl_sync(0xFFFFFFFFu, (unsigned long long)to_bits64<T>(v), src_lane));
+  else
+    return from_bits64<T>(__shfl_sync(0xFFFFFFFFu, (unsigned)to_bits64<T>(v), src_lane));
+}
+
+template <int KIND>
+constexpr bool kTwoInputs = KIND == kMismatch || KIND == kEqual || KIND == kLexicographic;
 
 __device__ __forceinline__ uint64_t pair_len(const Src& a, const Src& b) {
   const uint64_t la = src_len(a), lb = src_len(b);
   return la < lb ? la : lb;
 }
 
+// Whether item i qualifies, from its value x, its neighbour (the previous
+// item for is_sorted_until / is_partitioned, the next for adjacent_find) and
+// the right input's item y.
 template <class T, int KIND, int LESS>
+__device__ __forceinline__ bool qualifies(int pred, T x, T nb, T y) {
+  if constexpr (KIND == kFindIf) return pred_holds<T>(pred, x);
+  else if constexpr (KIND == kPartitioned) return pred_holds<T>(pred, x) && !pred_holds<T>(pred, nb);
+  else if constexpr (KIND == kAdjacentFind) return x == nb;
+  else if constexpr (KIND == kSortedUntil) return lt<T, LESS>(x, nb);
+  else if constexpr (KIND == kMismatch || KIND == kEqual) return !(x == y);
+  else return lt<T, LESS>(x, y) || lt<T, LESS>(y, x);
+}
+
+// KIND uses the previous item (+1 -> the next item, 0 -> none).
+template <int KIND>
+constexpr int kNeighbour = KIND == kAdjacentFind ? 1
+                           : (KIND == kSortedUntil || KIND == kPartitioned) ? -1 : 0;
+
+// One full tile of a plain column: the first qualifying index of this
+// thread's items, or kNone.
+template <class T, int KIND, int LESS>
+__device__ __forceinline__ uint32_t plain_tile(const T* __restrict__ a, const T* __restrict__ b,
+                                               uint64_t n, uint64_t base, int pred) {
+  using G = Geo<T>;
+  constexpr int NB = kNeighbour<KIND>;
+  T x[G::VECS][G::VEC], y[G::VECS][G::VEC];
+  load_vecs<T>(a, base, x);
+  if constexpr (kTwoInputs<KIND>) load_vecs<T>(b, base, y);
+  // neighbours across vector edges: the next lane's first item / the
+  // previous lane's last item; across warp edges, one scalar load
+  T edge[G::VECS];
+  const int lane = threadIdx.x & 31;
+  if constexpr (NB != 0) {
+#pragma unroll
+    for (int v = 0; v < G::VECS; ++v) {
+      if constexpr (NB > 0) {
+        edge[v] = shfl_t<T>(x[v][0], (lane + 1) & 31);
+        const uint64_t j = vec_index<T>(base, v, G::VEC - 1) + 1;
+        if (lane == 31 && j < n) edge[v] = a[j];
+      } else {
+        edge[v] = shfl_t<T>(x[v][G::VEC - 1], (lane + 31) & 31);
+        const uint64_t i0 = vec_index<T>(base, v, 0);
+        if (lane == 0 && i0 >= 1) edge[v] = a[i0 - 1];
+      }
+    }
+  }
+  uint32_t first = kNone;
+#pragma unroll
+  for (int v = 0; v < G::VECS; ++v) {
+#pragma unroll
+    for (int e = 0; e < G::VEC; ++e) {
+      const uint64_t i = vec_index<T>(base, v, e);
+      T nb = x[v][e];
+      if constexpr (NB > 0) nb = e + 1 < G::VEC ? x[v][e + 1] : edge[v];
+      if constexpr (NB < 0) nb = e > 0 ? x[v][e - 1] : edge[v];
+      bool ok = true;
+      if constexpr (NB > 0) ok = i + 1 < n;
+      if constexpr (NB < 0) ok = i >= 1;
+      const T yy = kTwoInputs<KIND> ? y[v][e] : x[v][e];
+      if (first == kNone && ok && qualifies<T, KIND, LESS>(pred, x[v][e], nb, yy))
+        first = (uint32_t)i;
+    }
+  }
+  return first;
+}
+
+// Any tile of any view (and the partial last tile of a plain column).
+template <class T, int KIND, int LESS>
+__device__ __forceinline__ uint32_t view_tile(const Src& a, const Src& b, uint64_t n,
+                                              uint64_t base, int pred) {
+  constexpr int NB = kNeighbour<KIND>;
+  uint32_t first = kNone;
+#pragma unroll 4
+  for (int j = 0; j < Geo<T>::ITEMS; ++j) {
+    const uint64_t i = base + (uint64_t)j * kThreads + threadIdx.x;
+    if (i >= n) break;
+    if constexpr (NB > 0) {
+      if (i + 1 >= n) continue;
+    }
+    if constexpr (NB < 0) {
+      if (i == 0) continue;
+    }
+    const T x = src_load<T>(a, i);
+    T nb = x, y = x;
+    if constexpr (NB != 0) nb = src_load<T>(a, NB > 0 ? i + 1 : i - 1);
+    if constexpr (kTwoInputs<KIND>) y = src_load<T>(b, i);
+    if (qualifies<T, KIND, LESS>(pred, x, nb, y)) {
+      first = (uint32_t)i;
+      break;
+    }
+  }
+  return first;
+}
+
+// Blocks walk tiles in increasing order, offer each tile's first hit to
+// `best` and stop once `best` lies before their next tile.  The barrier at
+// the top of every tile makes the exit block-uniform (and lets this block's
+// own hit, offered before it, end the walk).
+template <class T, int KIND, int LESS, bool PLAIN>
 __global__ void __launch_bounds__(kThreads)
     find_first_kernel(Src a, Src b, int pred, uint32_t* __restrict__ best) {
-  if constexpr (KIND == kFindIf) {
-    first_hit_tiles(src_len(a), best,
-                    [&](uint64_t i) { return pred_holds<T>(pred, src_load<T>(a, i)); });
-  } else if constexpr (KIND == kPartitioned) {
-    // the first passing item that follows a failing one
-    first_hit_tiles(src_len(a), best, [&](uint64_t i) {
-      return i >= 1 && pred_holds<T>(pred, src_load<T>(a, i)) &&
-             !pred_holds<T>(pred, src_load<T>(a, i - 1));
-    });
-  } else if constexpr (KIND == kAdjacentFind) {
-    const uint64_t n = src_len(a);
-    first_hit_tiles(n, best, [&](uint64_t i) {
-      return i + 1 < n && src_load<T>(a, i) == src_load<T>(a, i + 1);
-    });
-  } else if constexpr (KIND == kSortedUntil) {
-    first_hit_tiles(src_len(a), best, [&](uint64_t i) {
-      return i >= 1 && lt<T, LESS>(src_load<T>(a, i), src_load<T>(a, i - 1));
-    });
-  } else if constexpr (KIND == kMismatch || KIND == kEqual) {
-    first_hit_tiles(pair_len(a, b), best,
-                    [&](uint64_t i) { return !(src_load<T>(a, i) == src_load<T>(b, i)); });
-  } else {
-    first_hit_tiles(pair_len(a, b), best, [&](uint64_t i) {
-      const T x = src_load<T>(a, i), y = src_load<T>(b, i);
-      return lt<T, LESS>(x, y) || lt<T, LESS>(y, x);
-    });
+  using G = Geo<T>;
+  const uint64_t n = kTwoInputs<KIND> ? pair_len(a, b) : src_len(a);
+  for (uint64_t base = blockIdx.x * (uint64_t)G::TILE; base < n;
+       base += (uint64_t)gridDim.x * G::TILE) {
+    if (__syncthreads_or(base >= (uint64_t)ld_word(best))) return;
+    uint32_t first;
+    if (PLAIN && base + G::TILE <= n)
+      first = plain_tile<T, KIND, LESS>((const T*)a.data, (const T*)b.data, n, base, pred);
+    else
+      first = view_tile<T, KIND, LESS>(a, b, n, base, pred);
+    if (first != kNone) atomicMin(best, first);
+  }
+}
+
+// The walk of find_first_of (one item at a time; the needle loop dominates).
+template <class HIT>
+__device__ __forceinline__ void first_hit_tiles(uint64_t n, uint32_t* best, HIT hit) {
+  for (uint64_t base = blockIdx.x * (uint64_t)kTile; base < n;
+       base += (uint64_t)gridDim.x * kTile) {
+    if (__syncthreads_or(base >= (uint64_t)ld_word(best))) return;
+    uint32_t first = kNone;
+    for (int j = 0; j < kItems; ++j) {
+      const uint64_t i = base + (uint64_t)j * kThreads + threadIdx.x;
+      if (i < n && hit(i)) {
+        first = (uint32_t)i;
+        break;
+      }
+    }
+    if (first != kNone) atomicMin(best, first);
   }
 }
 
@@ -188,22 +307,25 @@ __global__ void find_finish_kernel(Src a, Src b, const uint32_t* __restrict__ be
   *out = r;
 }
 
-unsigned grid_of(mb_executor* ex, uint64_t n) {
+unsigned grid_of(mb_executor* ex, uint64_t n, uint64_t tile) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ex->device);
-  const uint64_t tiles = (n + kTile - 1) / kTile;
+  const uint64_t tiles = (n + tile - 1) / tile;
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)sms * 8));
 }
 
 template <class T, int KIND, int LESS>
-int find_launch(mb_executor* ex, const Src& a, const Src& b, uint64_t cap, int pred,
+int find_launch(mb_executor* ex, const Src& a, const Src& b, uint64_t cap, int pred, bool plain,
                 uint32_t* best, uint32_t* out) {
   if (cap) {
     if constexpr (KIND == kFirstOf) {
-      find_first_of_kernel<T><<<grid_of(ex, cap), kThreads, 0, ex->stream>>>(a, b, best);
+      find_first_of_kernel<T><<<grid_of(ex, cap, kTile), kThreads, 0, ex->stream>>>(a, b, best);
     } else {
-      find_first_kernel<T, KIND, LESS><<<grid_of(ex, cap), kThreads, 0, ex->stream>>>(a, b, pred,
-                                                                                    best);
+      const unsigned g = grid_of(ex, cap, Geo<T>::TILE);
+      if (plain)
+        find_first_kernel<T, KIND, LESS, true><<<g, kThreads, 0, ex->stream>>>(a, b, pred, best);
+      else
+        find_first_kernel<T, KIND, LESS, false><<<g, kThreads, 0, ex->stream>>>(a, b, pred, best);
     }
     MB_CUDA(cudaGetLastError());
   }
@@ -216,7 +338,11 @@ template <class T>
 int find_run(mb_executor* ex, int kind, const mb_src& a, const mb_src& b, uint64_t cap, int op,
              uint32_t* best, uint32_t* out) {
   const Src sa = to_src(a), sb = to_src(b);
-#define MB_FIND(K, L) return find_launch<T, K, L>(ex, sa, sb, cap, op, best, out)
+  constexpr int ct = DTypeOf<T>::value;
+  const bool two = kind == kMismatch || kind == kEqual || kind == kLexicographic;
+  const bool plain = src_plain(a, ct) && (uintptr_t)a.data % 16 == 0 &&
+                     (!two || (src_plain(b, ct) && (uintptr_t)b.data % 16 == 0));
+#define MB_FIND(K, L) return find_launch<T, K, L>(ex, sa, sb, cap, op, plain, best, out)
 #define MB_FIND_LESS(K)                            \
   switch (op) {                                    \
     case MB_GREATER: MB_FIND(K, MB_GREATER);       \
@@ -370,45 +496,56 @@ __device__ ArgAcc<T> block_combine(ArgAcc<T> acc) {
 // (the pass after the last NaN; the kernel returns at once if there was
 // none).  Partials per block: the minimum's and the maximum's value bits
 // (pv[2b], pv[2b+1]) and indices (pi[2b], pi[2b+1]).
+// Folds one item into a thread's accumulator; a thread's items arrive in
+// increasing index order.
 template <class T, int LESS, int KIND>
+__device__ __forceinline__ void arg_take(ArgAcc<T>& acc, T v, uint32_t i) {
+  constexpr bool kLast = KIND == kMinMax;
+  if constexpr (kNanAware<T, LESS>) {
+    if (v != v) {
+      acc.q = i + 1;
+      return;
+    }
+  }
+  if constexpr (KIND != kMaxFirst) {
+    if (acc.mn.i == kNone || lt<T, LESS>(v, acc.mn.v) || (kLast && !lt<T, LESS>(acc.mn.v, v)))
+      acc.mn = Cand<T>{v, i};
+  }
+  if constexpr (KIND != kMinFirst) {
+    if (acc.mx.i == kNone || lt<T, LESS>(acc.mx.v, v)) acc.mx = Cand<T>{v, i};
+  }
+}
+
+template <class T, int LESS, int KIND, bool PLAIN>
 __global__ void __launch_bounds__(kThreads)
     arg_partial_kernel(Src a, const uint32_t* __restrict__ lo_word, uint64_t* __restrict__ pv,
                        uint32_t* __restrict__ pi, uint32_t* __restrict__ q_word) {
-  constexpr bool kLast = KIND == kMinMax;
+  using G = Geo<T>;
   uint64_t lo = 0;
   if (lo_word) {
     lo = *lo_word;
     if (lo == 0) return;
   }
+  // vector loads need tiles that start on a 16-byte boundary
+  const bool vec = PLAIN && lo % G::VEC == 0;
   const uint64_t n = src_len(a);
   ArgAcc<T> acc{{T(0), kNone}, {T(0), kNone}, 0};
-  for (uint64_t base = lo + blockIdx.x * (uint64_t)kTile; base < n;
-       base += (uint64_t)gridDim.x * kTile) {
-    T v[kItems];
+  for (uint64_t base = lo + blockIdx.x * (uint64_t)G::TILE; base < n;
+       base += (uint64_t)gridDim.x * G::TILE) {
+    if (vec && base + G::TILE <= n) {
+      T x[G::VECS][G::VEC];
+      load_vecs<T>((const T*)a.data, base, x);
 #pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-      const uint64_t i = base + (uint64_t)j * kThreads + threadIdx.x;
-      v[j] = i < n ? src_load<T>(a, i) : T(0);
-    }
+      for (int v = 0; v < G::VECS; ++v)
 #pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-      const uint64_t i = base + (uint64_t)j * kThreads + threadIdx.x;
-      if (i >= n) break;
-      if constexpr (kNanAware<T, LESS>) {
-        if (v[j] != v[j]) {
-          acc.q = (uint32_t)i + 1;
-          continue;
-        }
-      }
-      // this thread's items arrive in increasing index order
-      const Cand<T> c{v[j], (uint32_t)i};
-      if constexpr (KIND != kMaxFirst) {
-        if (acc.mn.i == kNone || lt<T, LESS>(c.v, acc.mn.v) ||
-            (kLast && !lt<T, LESS>(acc.mn.v, c.v)))
-          acc.mn = c;
-      }
-      if constexpr (KIND != kMinFirst) {
-        if (acc.mx.i == kNone || lt<T, LESS>(acc.mx.v, c.v)) acc.mx = c;
+        for (int e = 0; e < G::VEC; ++e)
+          arg_take<T, LESS, KIND>(acc, x[v][e], (uint32_t)vec_index<T>(base, v, e));
+    } else {
+#pragma unroll 4
+      for (int j = 0; j < G::ITEMS; ++j) {
+        const uint64_t i = base + (uint64_t)j * kThreads + threadIdx.x;
+        if (i >= n) break;
+        arg_take<T, LESS, KIND>(acc, src_load<T>(a, i), (uint32_t)i);
       }
     }
   }
@@ -468,7 +605,8 @@ __global__ void __launch_bounds__(kThreads)
 
 template <class T, int LESS, int KIND>
 int arg_launch(mb_executor* ex, const mb_src& a, uint32_t* out) {
-  const unsigned g = grid_of(ex, a.len);
+  const unsigned g = grid_of(ex, a.len, Geo<T>::TILE);
+  const bool plain = src_plain(a, DTypeOf<T>::value) && (uintptr_t)a.data % 16 == 0;
   Scratch part;
   MB_TRY(part.alloc(ex, (size_t)g * 24 + 64));
   uint64_t* pv = part.as<uint64_t>();
@@ -477,11 +615,17 @@ int arg_launch(mb_executor* ex, const mb_src& a, uint32_t* out) {
   const Src s = to_src(a);
   constexpr bool kSecond = KIND == kMinMax && kNanAware<T, LESS>;
   if constexpr (kSecond) MB_CUDA(cudaMemsetAsync(q, 0, 4, ex->stream));
-  arg_partial_kernel<T, LESS, KIND><<<g, kThreads, 0, ex->stream>>>(s, nullptr, pv, pi,
-                                                                   kSecond ? q : nullptr);
+  if (plain)
+    arg_partial_kernel<T, LESS, KIND, true><<<g, kThreads, 0, ex->stream>>>(
+        s, nullptr, pv, pi, kSecond ? q : nullptr);
+  else
+    arg_partial_kernel<T, LESS, KIND, false><<<g, kThreads, 0, ex->stream>>>(
+        s, nullptr, pv, pi, kSecond ? q : nullptr);
   arg_final_kernel<T, LESS, KIND><<<1, kThreads, 0, ex->stream>>>(s, pv, pi, (int)g, nullptr, out);
   if constexpr (kSecond) {
-    arg_partial_kernel<T, LESS, kMinMax><<<g, kThreads, 0, ex->stream>>>(s, q, pv, pi, nullptr);
+    // (rare: only after a NaN; items one by one)
+    arg_partial_kernel<T, LESS, kMinMax, false><<<g, kThreads, 0, ex->stream>>>(s, q, pv, pi,
+                                                                               nullptr);
     arg_final_kernel<T, LESS, kMinMax><<<1, kThreads, 0, ex->stream>>>(s, pv, pi, (int)g, q, out);
   }
   MB_CUDA(cudaGetLastError());
