@@ -505,8 +505,9 @@ class SimpleWorkload(Workload):
     """A one-call step over resident inputs, reported in GB/s of its byte
     model: reduce (n * 4), merge of two sorted lists ((l + r) * 4 * 2),
     gather through a random permutation (n * 12: indices, the values they
-    pick, the output), find_if with no passing item (a full scan, n * 4) and
-    minmax_element over f32 normals (n * 4)."""
+    pick, the output), find_if with no passing item (a full scan, n * 4),
+    minmax_element over f32 normals (n * 4) and scatter_reduce of u32 adds
+    into 2^20 counters (n * 8 + 2^20 * 8)."""
 
     kernel = "single call"
 
@@ -517,6 +518,7 @@ class SimpleWorkload(Workload):
                      "gather": f"gather_u32_2^{lg}",
                      "lower_bound": f"lower_bound_u32_2^{lg}_in_2^24",
                      "find_if": f"find_if_u32_2^{lg}_no_hit",
+                     "scatter_reduce": f"scatter_reduce_add_u32_2^{lg}_into_2^20",
                      "minmax": f"minmax_element_f32_2^{lg}"}[kind]
         self.metric = f"{kind} GB/s"
         self.unit = "GB/s"
@@ -533,6 +535,10 @@ class SimpleWorkload(Workload):
         elif self.kind == "lower_bound":
             self.src = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 13, 1 << 24))
             self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 14, self.n)
+        elif self.kind == "scatter_reduce":
+            self.x = device_uniform_u32(ex, 0, 0xFFFF, 17, self.n)
+            self.idx = device_uniform_u32(ex, 0, (1 << 20) - 1, 18, self.n)
+            self.res = ex.alloc(np.uint32, 1 << 20)
         elif self.kind == "find_if":
             self.x = device_uniform_u32(ex, 1, 0xFFFFFFFF, 15, self.n)  # no zero: no hit
             self.res = ex.alloc(np.uint32, 2)
@@ -554,6 +560,8 @@ class SimpleWorkload(Workload):
             self.out = vector.merge(ex, self.a, self.b)
         elif self.kind == "lower_bound":
             self.out = vector.lower_bound(ex, self.src, self.x)
+        elif self.kind == "scatter_reduce":
+            vector.scatter_reduce(ex, self.x, self.idx, np.uint32(0), op.Add, self.res)
         elif self.kind == "find_if":
             vector.find_if(ex, self.x, "is_false", out=self.res)
         elif self.kind == "minmax":
@@ -567,6 +575,8 @@ class SimpleWorkload(Workload):
     def alg_bytes(self):
         # lower_bound: each query's value in and index out (the 64 MB source
         # stays in L2 after the first probes)
+        if self.kind == "scatter_reduce":  # value + index per proposal, 2^20 counters r+w
+            return 8.0 * self.n + 8.0 * (1 << 20)
         return {"reduce": 4.0, "merge": 8.0, "gather": 12.0, "lower_bound": 8.0, "find_if": 4.0,
                 "minmax": 4.0}[self.kind] * self.n
 
@@ -598,12 +608,13 @@ WORKLOADS = {
     "gather_u32": lambda: SimpleWorkload("gather", _n(28)),
     "lower_bound_u32": lambda: SimpleWorkload("lower_bound", _n(26)),
     "find_if_u32": lambda: SimpleWorkload("find_if", _n(28)),
+    "scatter_reduce_u32": lambda: SimpleWorkload("scatter_reduce", _n(28)),
     "minmax_element_f32": lambda: SimpleWorkload("minmax", _n(28)),
 }
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64",
              "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by", "reduce_u32",
              "merge_u32", "gather_u32", "lower_bound_u32", "find_if_u32",
-             "minmax_element_f32"]
+             "minmax_element_f32", "scatter_reduce_u32"]
 
 
 # -------------------------------------------------------------- helpers --

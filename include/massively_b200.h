@@ -275,6 +275,18 @@ int mb_gather(mb_executor* exec, const mb_src* values, const mb_src* indices,
  * Colliding indices leave one unspecified writer, as in massively. */
 int mb_scatter(mb_executor* exec, const mb_src* values, const mb_src* indices,
                const mb_src* stencil, mb_col out);
+/* vector::scatter_reduce (massively/src/api/algorithm/scatter.rs:332-420;
+ * core massively/src/core/scatter_reduce.rs): for every destination d named
+ * by `indices`, out[c][d] = out[c][d] op[c] (inits[c] op[c] v_1 op[c] ...),
+ * per value column c; other destinations keep their value.  Each op must be
+ * associative and commutative (not TAKE_LEFT / TAKE_RIGHT); values[c] and
+ * out[c] have the same element type; `inits` holds one 8-byte slot per
+ * column (value bits in the low bytes).  Proposals of one destination are
+ * combined in an unspecified order (float ADD may round differently from run
+ * to run).  An index at or past out[c].len is skipped and reported as a launch
+ * error at the next synchronisation. */
+int mb_scatter_reduce(mb_executor* exec, const mb_src* values, int nvals, const mb_src* indices,
+                      const int* ops, const uint64_t* inits, const mb_col* out);
 
 /* ---------------------------------------------------------- ordering ---- */
 

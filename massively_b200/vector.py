@@ -307,6 +307,26 @@ def _scatter_into(exec, values, indices, stencil, outs):
                               C.byref(st) if st is not None else None, o.to_col()))
 
 
+def scatter_reduce(exec: Executor, values, indices, init, op, output) -> None:
+    """vector::scatter_reduce (massively/src/api/algorithm/scatter.rs:377):
+    out[d] = out[d] op (init op v ...) for every destination named by
+    `indices`; other destinations keep their value.  `op` must be associative
+    and commutative; for zipped values / outputs `op` and `init` may be
+    per-column tuples."""
+    _check_owner(exec, values, indices, output)
+    n, m = _len(values), _len(indices)
+    if n != m:
+        raise LengthMismatch(n, m)
+    keep = []
+    vs, nv = _srcs(exec, values, keep)
+    ix = lower(exec, indices, keep)
+    outs = _columns(output)
+    if len(outs) != nv:
+        raise LengthMismatch(nv, len(outs))
+    ids, bits = _ops_inits(values, op, init)
+    check(_L().mb_scatter_reduce(exec.handle, vs, nv, C.byref(ix), ids, bits, _cols(outs)))
+
+
 def reverse(exec: Executor, values):
     """vector::reverse (indexed.rs:289)."""
     from .lazy import Reverse

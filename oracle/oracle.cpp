@@ -466,6 +466,28 @@ template <class T> int arg_t(int kind, const void* in, uint64_t n, int less, uin
   return 0;
 }
 
+// scatter_reduce: massively/src/api/algorithm/scatter.rs:332-420 with
+// core/scatter_reduce.rs:179.  Proposals are taken in input order (the
+// stable index sort of the reference keeps it): for every destination d,
+// acc = init op v_1 op ... op v_k, then out[d] = out[d] op acc.  Indices past
+// the output are skipped.
+template <class T> int scatter_reduce_t(const void* vals, const uint32_t* idx, uint64_t n,
+                                        int op, const void* init, void* out, uint64_t nout) {
+  const T* v = (const T*)vals; T* o = (T*)out;
+  const T in = *(const T*)init;
+  std::vector<T> acc(nout);
+  std::vector<char> has(nout, 0);
+  for (uint64_t i = 0; i < n; ++i) {
+    const uint64_t d = idx[i];
+    if (d >= nout) continue;
+    acc[d] = has[d] ? apply_op<T>(op, acc[d], v[i]) : apply_op<T>(op, in, v[i]);
+    has[d] = 1;
+  }
+  for (uint64_t d = 0; d < nout; ++d)
+    if (has[d]) o[d] = apply_op<T>(op, o[d], acc[d]);
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -628,6 +650,11 @@ int64_t orc_set_op_src(int dt, const void* l, uint64_t nl, const void* r, uint64
 int orc_bounds(int dt, const void* src, uint64_t n, const void* vals, uint64_t m, int less,
                int upper, uint32_t* out) {
   ORC_DISPATCH(dt, bounds_t, src, n, vals, m, less, upper, out);
+  return -1;
+}
+int orc_scatter_reduce(int dt, const void* vals, const uint32_t* idx, uint64_t n, int op,
+                       const void* init, void* out, uint64_t nout) {
+  ORC_DISPATCH(dt, scatter_reduce_t, vals, idx, n, op, init, out, nout);
   return -1;
 }
 int64_t orc_find(int kind, int dt, const void* a, uint64_t na, const void* b, uint64_t nb,

@@ -76,6 +76,7 @@ def _declare(L: C.CDLL) -> None:
         "orc_set_op_src": (i64, [i32, vp, u64, vp, u64, i32, i32, vp]),
         "orc_unique": (i64, [i32, vp, u64, i32, vp]),
         "orc_find": (i64, [i32, i32, vp, u64, vp, u64, i32]),
+        "orc_scatter_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp, u64]),
         "orc_arg": (i32, [i32, i32, vp, u64, i32, vp]),
         "orc_seg_scan": (i32, [i32, vp, vp, u64, i32, i32, vp, vp]),
         "orc_seg_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp]),
@@ -451,6 +452,20 @@ def unique(x, eq: str = "equal") -> np.ndarray:
 
 
 # --------------------------------------------------------------------- seg --
+
+def scatter_reduce(values, indices, init, op: str, out):
+    """massively/src/api/algorithm/scatter.rs:332-420: out[d] op (init op
+    v ...) per destination, proposals in input order; returns a new array."""
+    values, indices = _c(values), _c(indices).astype(np.uint32)
+    o = np.array(out, copy=True)
+    if o.dtype != values.dtype:
+        raise TypeError("output element type differs from the values'")
+    iv = _scalar(init, values.dtype)
+    if lib().orc_scatter_reduce(_dt(values), _p(values), _p(indices), values.size, OPS[op],
+                                _p(iv), _p(o), o.size) != 0:
+        raise TypeError(values.dtype)
+    return o
+
 
 NONE = 0xFFFFFFFF  # MIndex::MAX, massively's None
 

@@ -281,6 +281,29 @@ PREDICATES = [
          a=np.array([1, 2, 3], U32), b=np.array([1, 3, 0], U32), arg="less", want=True),
 ]
 
+# scatter_reduce: the doctest of massively/src/api/algorithm/scatter.rs and
+# its unit tests (multi-column rows, component-wise add).  `values` /
+# `output` are lists of columns; `want` the outputs after the call.
+SCATTER_REDUCE = [
+    dict(src="massively/src/api/algorithm/scatter.rs:361-375",
+         values=[np.array([2, 3, 5, 7], U32)], indices=np.array([1, 0, 1, 1], U32),
+         init=[0], op="add", output=[np.array([10, 20, 30], U32)],
+         want=[np.array([13, 34, 30], U32)]),
+    dict(src="massively/src/api/algorithm/scatter.rs:447-466",
+         values=[np.array([1, 2, 3], U32), np.array([10, 20, 30], U32)],
+         indices=np.array([1, 0, 1], U32), init=[0, 0], op="add",
+         output=[np.array([100, 200], U32), np.array([1000, 2000], U32)],
+         want=[np.array([102, 204], U32), np.array([1020, 2040], U32)]),
+    dict(src="massively/src/api/algorithm/scatter.rs:469-495",
+         values=[np.array([1, 2, 3], U32), np.array([10, 20, 30], U32),
+                 np.array([100, 200, 300], U32)],
+         indices=np.array([1, 0, 1], U32), init=[0, 0, 0], op="add",
+         output=[np.array([100, 200], U32), np.array([1000, 2000], U32),
+                 np.array([10000, 20000], U32)],
+         want=[np.array([102, 204], U32), np.array([1020, 2040], U32),
+               np.array([10200, 20400], U32)]),
+]
+
 # massively/tests/vector/api/predicate.rs:17-22: count_if over a lazy
 # counting view of four billion items (u32 lengths above i32::MAX).
 COUNT_IF_FOUR_BILLION = dict(src="massively/tests/vector/api/predicate.rs:17-22",

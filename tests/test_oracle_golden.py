@@ -186,6 +186,21 @@ def test_predicate_edges(orc):
     assert orc.count_if(x, "is_odd") == int((x % 2 == 1).sum())
 
 
+def test_scatter_reduce_known_answers(orc):
+    for case in K.SCATTER_REDUCE:
+        for v, init, out, want in zip(case["values"], case["init"], case["output"], case["want"]):
+            got = orc.scatter_reduce(v, case["indices"], init, case["op"], out)
+            np.testing.assert_array_equal(got, want, err_msg=case["src"])
+    # a non-identity init is folded in once per destination that received a
+    # proposal; untouched destinations keep their value
+    got = orc.scatter_reduce(np.array([1, 2, 3], np.int32), np.array([0, 0, 2], np.uint32), 100,
+                             "add", np.array([5, 6, 7], np.int32))
+    np.testing.assert_array_equal(got, [108, 6, 110])
+    got = orc.scatter_reduce(np.array([4, 9], np.uint8), np.array([1, 1], np.uint32), 255, "min",
+                             np.array([7, 7], np.uint8))
+    np.testing.assert_array_equal(got, [7, 4])
+
+
 def test_seg_known_answers(orc):
     for case in K.SEG:
         if case["kind"] == "reduce":
