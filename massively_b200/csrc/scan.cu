@@ -26,6 +26,7 @@
 // association is a fixed tree inside the tile plus the deterministic fold
 // across tiles, so results are identical run to run.
 
+#include <algorithm>
 #include <mutex>
 
 #include "bulk.cuh"
@@ -49,16 +50,24 @@ struct ScanCfg {
   static constexpr int TILE = kThreads * ITEMS;
 };
 
-template <class T>
-struct SmemCfg {
-  // Floats take 64 KB tiles: their deterministic look-back folds one
-  // aggregate per tile in sequence, so fewer, larger tiles shorten that chain.
-  static constexpr int ROWS = std::is_floating_point<T>::value ? 2 * kRows : kRows;
+template <class T, int R>
+struct TileCfg {
+  static constexpr int ROWS = R;
   static constexpr int VEC = 16 / sizeof(T);
   static constexpr int WARP_ITEMS = 32 * ROWS * VEC;
-  static constexpr int TILE = kWarps * WARP_ITEMS;  // 32 KB (64 KB for floats)
+  static constexpr int TILE = kWarps * WARP_ITEMS;
   static constexpr int TILE_BYTES = TILE * (int)sizeof(T);
 };
+
+// One-tile-per-CTA kernel.  Floats take 64 KB tiles: their deterministic
+// look-back folds one aggregate per tile in sequence, so fewer, larger tiles
+// shorten that chain.
+template <class T>
+struct SmemCfg : TileCfg<T, std::is_floating_point<T>::value ? 2 * kRows : kRows> {};
+
+// Alternative shape for the autotuner: 64 KB tiles for every type.
+template <class T>
+struct BigCfg : TileCfg<T, 2 * kRows> {};
 
 template <class T>
 struct ScanParams {
@@ -122,45 +131,12 @@ __device__ __forceinline__ void tile_prefixes(uint64_t tile, const ScanParams<T>
   }
 }
 
-template <class T, int OP, bool PACKED>
-__global__ void __launch_bounds__(kThreads)
-    scan_smem_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
-                     ScanParams<T> p, TileState<T, PACKED> st) {
-  using C = SmemCfg<T>;
+// Phase 1 of one tile held in `buf`: warp-local inclusive scan, row by row,
+// in place; the warp totals go to s_wtot.  (No barrier inside.)
+template <class T, int OP, class C>
+__device__ __forceinline__ void smem_phase1(T* buf, const ScanParams<T>& p, T* s_wtot) {
   constexpr int VEC = C::VEC;
-  extern __shared__ __align__(128) unsigned char scan_smem[];
-  T* buf = reinterpret_cast<T*>(scan_smem);
-  __shared__ __align__(8) uint64_t bar;
-  __shared__ uint32_t s_tile;
-  __shared__ T s_wtot[kWarps];
-  __shared__ T s_pre[kWarps];
-  __shared__ bool s_has[kWarps];
-
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    const uint32_t t = atomicAdd(p.counter, 1u);
-    s_tile = t;
-    mbar_init(&bar, 1);
-    mbar_init_fence();
-    if ((uint64_t)(t + 1) * C::TILE <= n) {
-      mbar_arrive_expect_tx(&bar, C::TILE_BYTES);
-      bulk_load(buf, in + (uint64_t)t * C::TILE, C::TILE_BYTES, &bar);
-    }
-  }
-  __syncthreads();
-  const uint64_t tile = s_tile;
-  const uint64_t tile_base = tile * (uint64_t)C::TILE;
-  if (tile_base >= n) return;
-  const bool full = tile_base + C::TILE <= n;
-  if (full) {
-    if (!mbar_wait(&bar, 0)) raise_device_error(p.err, MB_DEV_ERR_LOOKBACK);
-  } else {
-    for (int i = threadIdx.x; i < C::TILE; i += kThreads)
-      buf[i] = tile_base + i < n ? in[tile_base + i] : T(0);
-    __syncthreads();
-  }
-
-  // Phase 1: warp-local inclusive scan, row by row, in place.
   const Op<T, OP> op{p.op};
   T* wb = buf + warp * C::WARP_ITEMS;
   T carry = T(0);
@@ -191,16 +167,21 @@ __global__ void __launch_bounds__(kThreads)
     carry = j > 0 ? op(carry, rowtot) : rowtot;
   }
   if (lane == 0) s_wtot[warp] = carry;
-  __syncthreads();
+}
 
-  // Phase 2: tile aggregate, look-back, warp prefixes.
-  if (warp == 0) tile_prefixes<T, OP, PACKED>(tile, p, st, s_wtot, s_pre, s_has);
-  __syncthreads();
-
-  // Phase 3: apply the warp prefix on the way out.
+// Phase 3: every value combined with its warp prefix on the way out; `full`
+// tiles store 16-byte vectors, the last, partial tile item by item.
+template <class T, int OP, class C>
+__device__ __forceinline__ void smem_phase3(const T* buf, uint64_t tile, uint64_t n, bool full,
+                                            T* __restrict__ out, const ScanParams<T>& p,
+                                            const T* s_pre, const bool* s_has) {
+  constexpr int VEC = C::VEC;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const Op<T, OP> op{p.op};
+  const T* wb = buf + warp * C::WARP_ITEMS;
   const T pre = s_pre[warp];
   const bool has = s_has[warp];
-  const uint64_t wg = tile_base + (uint64_t)warp * C::WARP_ITEMS;
+  const uint64_t wg = tile * (uint64_t)C::TILE + (uint64_t)warp * C::WARP_ITEMS;
 #pragma unroll 2
   for (int j = 0; j < C::ROWS; ++j) {
     const int li = (j * 32 + lane) * VEC;  // warp-local index of item 0
@@ -231,6 +212,142 @@ __global__ void __launch_bounds__(kThreads)
         if (wg + li + k < n) out[wg + li + k] = o[k];
     }
   }
+}
+
+// Phases 1-3 of one tile, warp 0 running the look-back between them.
+template <class T, int OP, bool PACKED, class C>
+__device__ __forceinline__ void smem_tile(T* buf, uint64_t tile, uint64_t n, bool full,
+                                          T* __restrict__ out, const ScanParams<T>& p,
+                                          const TileState<T, PACKED>& st, T* s_wtot, T* s_pre,
+                                          bool* s_has) {
+  smem_phase1<T, OP, C>(buf, p, s_wtot);
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) tile_prefixes<T, OP, PACKED>(tile, p, st, s_wtot, s_pre, s_has);
+  __syncthreads();
+  smem_phase3<T, OP, C>(buf, tile, n, full, out, p, s_pre, s_has);
+}
+
+template <class T, int OP, bool PACKED, class C>
+__global__ void __launch_bounds__(kThreads)
+    scan_smem_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
+                     ScanParams<T> p, TileState<T, PACKED> st) {
+  extern __shared__ __align__(128) unsigned char scan_smem[];
+  T* buf = reinterpret_cast<T*>(scan_smem);
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t s_tile;
+  __shared__ T s_wtot[kWarps];
+  __shared__ T s_pre[kWarps];
+  __shared__ bool s_has[kWarps];
+
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(p.counter, 1u);
+    s_tile = t;
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+    if ((uint64_t)(t + 1) * C::TILE <= n) {
+      mbar_arrive_expect_tx(&bar, C::TILE_BYTES);
+      bulk_load(buf, in + (uint64_t)t * C::TILE, C::TILE_BYTES, &bar);
+    }
+  }
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t tile_base = tile * (uint64_t)C::TILE;
+  if (tile_base >= n) return;
+  const bool full = tile_base + C::TILE <= n;
+  if (full) {
+    if (!mbar_wait(&bar, 0)) raise_device_error(p.err, MB_DEV_ERR_LOOKBACK);
+  } else {
+    for (int i = threadIdx.x; i < C::TILE; i += kThreads)
+      buf[i] = tile_base + i < n ? in[tile_base + i] : T(0);
+    __syncthreads();
+  }
+  smem_tile<T, OP, PACKED, C>(buf, tile, n, full, out, p, st, s_wtot, s_pre, s_has);
+}
+
+// Barrier among the first `count` threads (ids 1..15; 0 is __syncthreads).
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// The same tile scan with a ninth warp that runs the look-back while the
+// bulk load lands and the eight compute warps scan their rows, so the
+// look-back's L2 round trips leave the tile's critical path: by the time the
+// tile's own aggregate is known its exclusive prefix usually is too.  The
+// compute warps publish the aggregate after phase 1 and the inclusive prefix
+// after joining the look-back warp.  (The look-back never needs the tile's
+// own aggregate; the fold order is the same as warp 0's, so float results
+// are unchanged.)
+template <class T, int OP, bool PACKED, class C>
+__global__ void __launch_bounds__(kThreads + 32)
+    scan_smem_lb_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
+                        ScanParams<T> p, TileState<T, PACKED> st) {
+  constexpr bool DET = std::is_floating_point<T>::value;
+  extern __shared__ __align__(128) unsigned char scan_smem[];
+  T* buf = reinterpret_cast<T*>(scan_smem);
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t s_tile;
+  __shared__ T s_wtot[kWarps];
+  __shared__ T s_pre[kWarps];
+  __shared__ bool s_has[kWarps];
+  __shared__ T s_excl;
+
+  const int warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(p.counter, 1u);
+    s_tile = t;
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+    if ((uint64_t)(t + 1) * C::TILE <= n) {
+      mbar_arrive_expect_tx(&bar, C::TILE_BYTES);
+      bulk_load(buf, in + (uint64_t)t * C::TILE, C::TILE_BYTES, &bar);
+    }
+  }
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t tile_base = tile * (uint64_t)C::TILE;
+  if (tile_base >= n) return;
+  const bool full = tile_base + C::TILE <= n;
+  const Op<T, OP> op{p.op};
+  if (warp == kWarps) {
+    // the look-back warp
+    T excl = T(0);
+    if (tile > 0) excl = lookback_exclusive<T, Op<T, OP>, DET>(st, tile, op, p.err, T(0));
+    if ((threadIdx.x & 31) == 0) s_excl = excl;
+  } else {
+    if (full) {
+      if (!mbar_wait(&bar, 0)) raise_device_error(p.err, MB_DEV_ERR_LOOKBACK);
+    } else {
+      for (int i = threadIdx.x; i < C::TILE; i += kThreads)
+        buf[i] = tile_base + i < n ? in[tile_base + i] : T(0);
+      named_sync(1, kThreads);
+    }
+    smem_phase1<T, OP, C>(buf, p, s_wtot);
+    named_sync(1, kThreads);
+    if (threadIdx.x == 0) {
+      T agg = s_wtot[0];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) agg = op(agg, s_wtot[w]);
+      st.publish(tile, tile == 0 ? kFlagIncl : kFlagAgg, agg);
+    }
+  }
+  __syncthreads();  // s_excl and s_wtot are ready
+  if (warp == kWarps) return;
+  if (threadIdx.x == 0) {
+    const T excl = s_excl;
+    bool h = tile > 0;
+    T acc = excl;
+    T agg = s_wtot[0];
+    for (int w = 0; w < kWarps; ++w) {
+      s_pre[w] = acc;
+      s_has[w] = h;
+      acc = h ? op(acc, s_wtot[w]) : s_wtot[w];
+      h = true;
+      if (w > 0) agg = op(agg, s_wtot[w]);
+    }
+    if (tile > 0) st.publish(tile, kFlagIncl, op(excl, agg));
+  }
+  named_sync(1, kThreads);
+  smem_phase3<T, OP, C>(buf, tile, n, full, out, p, s_pre, s_has);
 }
 
 // Register-tiled scan of one tile held in x (warp-striped vectors) into its
@@ -395,7 +512,11 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
   const bool plain = src_plain(in, DTypeOf<T>::value) && out.dtype == DTypeOf<T>::value &&
                      ((uintptr_t)in.data % 16 == 0) && ((uintptr_t)out.data % 16 == 0);
   const bool smem_path = plain && in.len_dev == nullptr;
-  const uint64_t tile_items = smem_path ? SmemCfg<T>::TILE : ScanCfg<T>::TILE;
+  const int shape = smem_path ? std::max(0, ex->tune[MB_TUNE_SCAN]) : 0;
+  // shapes: 0 = look-back warp, default tile; 1 = warp 0 runs the look-back,
+  // default tile; 2 = look-back warp, 64 KB tiles
+  const uint64_t tile_items = !smem_path ? ScanCfg<T>::TILE
+                              : shape == 2 ? BigCfg<T>::TILE : SmemCfg<T>::TILE;
   const uint64_t tiles = (cap + tile_items - 1) / tile_items;
   Scratch scratch;
   const size_t state_bytes = TileState<T, PACKED>::bytes(tiles);
@@ -412,15 +533,32 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
   auto st = TileState<T, PACKED>::make(scratch.as<char>() + 256, tiles);
   const Src s = to_src(in);
   dim3 grid(grid_for(tiles)), block(kThreads);
-  const size_t smem = SmemCfg<T>::TILE_BYTES;
+  const size_t smem = shape == 2 ? BigCfg<T>::TILE_BYTES : SmemCfg<T>::TILE_BYTES;
+#define MB_SCAN_SMEM(OPID, CFG)                                                             \
+  do {                                                                                      \
+    if (smem > 48 * 1024)                                                                   \
+      MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED, CFG>,                  \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    scan_smem_kernel<T, OPID, PACKED, CFG><<<grid, block, smem, ex->stream>>>(              \
+        (const T*)in.data, (T*)out.data, cap, p, st);                                       \
+  } while (0)
+#define MB_SCAN_LB(OPID, CFG)                                                               \
+  do {                                                                                      \
+    if (smem > 48 * 1024)                                                                   \
+      MB_CUDA(cudaFuncSetAttribute(scan_smem_lb_kernel<T, OPID, PACKED, CFG>,               \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    scan_smem_lb_kernel<T, OPID, PACKED, CFG><<<grid, kThreads + 32, smem, ex->stream>>>(   \
+        (const T*)in.data, (T*)out.data, cap, p, st);                                       \
+  } while (0)
 #define MB_SCAN_LAUNCH(OPID)                                                                    \
   do {                                                                                          \
     if (smem_path) {                                                                            \
-      if (smem > 48 * 1024)                                                                     \
-        MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED>,                         \
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
-      scan_smem_kernel<T, OPID, PACKED><<<grid, block, smem, ex->stream>>>(                     \
-          (const T*)in.data, (T*)out.data, cap, p, st);                                         \
+      if (shape == 1)                                                                           \
+        MB_SCAN_SMEM(OPID, SmemCfg<T>);                                                         \
+      else if (shape == 2)                                                                      \
+        MB_SCAN_LB(OPID, BigCfg<T>);                                                            \
+      else                                                                                      \
+        MB_SCAN_LB(OPID, SmemCfg<T>);                                                           \
     } else if (plain) {                                                                         \
       scan_kernel<T, OPID, true, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
     } else {                                                                                    \
@@ -435,6 +573,8 @@ int scan_run(mb_executor* ex, const mb_src& in, int op, bool exclusive, const vo
     default: MB_SCAN_LAUNCH(kOpDyn); break;
   }
 #undef MB_SCAN_LAUNCH
+#undef MB_SCAN_SMEM
+#undef MB_SCAN_LB
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -541,9 +681,9 @@ int scan_noalloc_run(mb_executor* ex, const mb_src& in, int op, const mb_col& ou
   do {                                                                                          \
     if (smem_path) {                                                                            \
       if (smem > 48 * 1024)                                                                     \
-        MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED>,                         \
+        MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED, SmemCfg<T>>,                         \
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
-      scan_smem_kernel<T, OPID, PACKED><<<grid, block, smem, ex->stream>>>(                     \
+      scan_smem_kernel<T, OPID, PACKED, SmemCfg<T>><<<grid, block, smem, ex->stream>>>(                     \
           (const T*)in.data, (T*)out.data, cap, p, st);                                         \
     } else if (plain) {                                                                         \
       scan_kernel<T, OPID, true, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \

@@ -16,16 +16,21 @@ extern "C" {
 int mb_tune_config_count(int family) {
   switch (family) {
     case MB_TUNE_RADIX: return radix_tune_count();
-    case MB_TUNE_SCAN: case MB_TUNE_REDUCE: case MB_TUNE_SELECT: return 1;
+    case MB_TUNE_SCAN: return 3;
+    case MB_TUNE_REDUCE: case MB_TUNE_SELECT: return 1;
     default: return 0;
   }
 }
 
 const char* mb_tune_describe(int family, int config) {
   if (family == MB_TUNE_RADIX) return radix_tune_text(config);
+  if (family == MB_TUNE_SCAN && config == 1)
+    return "scan one 32 KB tile per CTA, warp 0 runs the look-back after the tile scan";
+  if (family == MB_TUNE_SCAN && config == 2)
+    return "scan one 64 KB tile per CTA, a ninth warp runs the look-back";
   if (config == 0) {
     switch (family) {
-      case MB_TUNE_SCAN: return "scan 256 threads x 4 x 16-byte vectors per thread";
+      case MB_TUNE_SCAN: return "scan one 32 KB tile per CTA, a ninth warp runs the look-back";
       case MB_TUNE_REDUCE: return "reduce 256 threads x 4 x 16-byte vectors, fixed grid";
       case MB_TUNE_SELECT: return "compaction 256 threads x 16 items";
       default: break;

@@ -111,3 +111,34 @@ def test_unaligned_slice_and_errors(ex):
     assert e.value == mb.OutputTooShort(10_001, 10)
     empty = ex.to_device(np.zeros(0, np.uint32))
     assert ex.to_host(vector.inclusive_scan(ex, empty, op.Add)).size == 0
+
+
+@pytest.mark.parametrize("n", [1, 8191, 8192, 8193, 100_003, 1 << 22, (1 << 24) + 5])
+@pytest.mark.parametrize("dtype", [np.uint32, np.int64, np.float32, np.float64])
+def test_every_scan_config(n, dtype):
+    """Each scan configuration the autotuner may choose (the one-tile-per-CTA
+    kernel and the persistent double-buffered one) gives the same results:
+    bit-exact for integers, identical bits across configurations for floats
+    of the same tile shape, within the bound otherwise."""
+    from massively_b200 import op, tune, vector
+    ex = executor()
+    x = seeded(dtype, n, seed=n + 11)
+    d = ex.to_device(x)
+    for cfg in range(len(tune.configs("scan"))):
+        tune.set_config(ex, "scan", cfg)
+        inc = ex.to_host(vector.inclusive_scan(ex, d, op.Add))
+        exc = ex.to_host(vector.exclusive_scan(ex, d, dtype(3), op.Add))
+        mx = ex.to_host(vector.inclusive_scan(ex, d, op.Max))
+        np.testing.assert_array_equal(mx, orc.inclusive_scan(x, "max"), err_msg=f"config {cfg}")
+        if np.dtype(dtype).kind == "f":
+            exact = np.cumsum(x.astype(np.float64))
+            eps = 2.0 ** -24 if dtype == np.float32 else 2.0 ** -53
+            bound = (np.arange(n) + 1) * eps * np.cumsum(np.abs(x.astype(np.float64)))
+            assert (np.abs(inc.astype(np.float64) - exact) <= bound + 1e-30).all(), cfg
+            again = ex.to_host(vector.inclusive_scan(ex, d, op.Add))
+            np.testing.assert_array_equal(inc.view(np.uint8), again.view(np.uint8))
+        else:
+            np.testing.assert_array_equal(inc, orc.inclusive_scan(x, "add"), err_msg=f"config {cfg}")
+            np.testing.assert_array_equal(exc, orc.exclusive_scan(x, "add", dtype(3)),
+                                          err_msg=f"config {cfg}")
+    ex.sync()
