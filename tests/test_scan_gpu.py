@@ -116,10 +116,10 @@ def test_unaligned_slice_and_errors(ex):
 @pytest.mark.parametrize("n", [1, 8191, 8192, 8193, 100_003, 1 << 22, (1 << 24) + 5])
 @pytest.mark.parametrize("dtype", [np.uint32, np.int64, np.float32, np.float64])
 def test_every_scan_config(n, dtype):
-    """Each scan configuration the autotuner may choose (the one-tile-per-CTA
-    kernel and the persistent double-buffered one) gives the same results:
-    bit-exact for integers, identical bits across configurations for floats
-    of the same tile shape, within the bound otherwise."""
+    """Each scan configuration the autotuner may choose (one tile per CTA
+    with a look-back warp; the same with warp 0 running the look-back; 64 KB
+    tiles) gives the same results: bit-exact for integers and MAX; for float
+    ADD within the bound and identical run to run."""
     from massively_b200 import op, tune, vector
     ex = executor()
     x = seeded(dtype, n, seed=n + 11)
