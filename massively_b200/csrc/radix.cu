@@ -143,6 +143,82 @@ __global__ void __launch_bounds__(kHistThreads, 2)
   }
 }
 
+// The same counts with lane-private bins, for up to four passes (keys of up
+// to 32 bits): bin b of pass p is counted at word (p * kBins + b) * 32 + lane,
+// so the 32 atomics of one warp instruction always fall in 32 different
+// banks and never on one address -- no bank conflicts, whatever the digits.
+// 32 KB of counters per pass; one 1024-thread block per SM.
+constexpr int kHistLaneThreads = 1024;
+
+template <class K, int ENC, int PASSES>
+__global__ void __launch_bounds__(kHistLaneThreads, 1)
+    radix_histogram_lanes_kernel(const K* __restrict__ keys, uint64_t n,
+                                 const uint32_t* __restrict__ n_dev, uint32_t* __restrict__ hist) {
+  static_assert(PASSES <= 4, "lane-private bins for up to four passes");
+  if (n_dev && *n_dev < n) n = *n_dev;
+  constexpr int KPV = 16 / (int)sizeof(K);
+  constexpr int KPL = KPV * kHistUnroll;
+  constexpr uint64_t KPW = 32ull * KPL;
+  extern __shared__ __align__(16) uint32_t lanes_sh[];  // [PASSES][kBins][32]
+  for (int i = threadIdx.x; i < PASSES * kBins * 32; i += kHistLaneThreads) lanes_sh[i] = 0;
+  __syncthreads();
+  const uint32_t lane = lane_id();
+  uint32_t* mine = lanes_sh + lane;
+  const uint64_t warps = (uint64_t)gridDim.x * (kHistLaneThreads / 32);
+  const uint64_t gw = (uint64_t)blockIdx.x * (kHistLaneThreads / 32) + (threadIdx.x >> 5);
+  const uint64_t chunks = ((uintptr_t)keys & 15) == 0 ? n / KPW : 0;
+  for (uint64_t c = gw; c < chunks; c += warps) {
+    const uint4* src = reinterpret_cast<const uint4*>(keys + c * KPW);
+    uint4 v[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) v[u] = __ldcs(src + u * 32 + lane);
+    K k[KPL];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) {
+      const K* kv = reinterpret_cast<const K*>(&v[u]);
+#pragma unroll
+      for (int j = 0; j < KPV; ++j) k[u * KPV + j] = enc_bits<K, ENC>(kv[j]);
+    }
+    K any = 0, all = ~(K)0;
+#pragma unroll
+    for (int j = 0; j < KPL; ++j) {
+      any |= k[j];
+      all &= k[j];
+    }
+    const K ref = __shfl_sync(kFull, k[0], 0);
+    const K diff = (any ^ all) | (k[0] ^ ref);
+    const K wdiff = (K)__reduce_or_sync(kFull, (uint32_t)diff);
+#pragma unroll
+    for (int p = 0; p < PASSES; ++p) {
+      const int s = p * kRadixBits;
+      if (((wdiff >> s) & (kBins - 1)) == 0) {  // warp-uniform
+        if (lane == 0)
+          atomicAdd(mine + (p * kBins + ((uint32_t)(ref >> s) & (kBins - 1))) * 32, (uint32_t)KPW);
+      } else {
+#pragma unroll
+        for (int j = 0; j < KPL; ++j)
+          atomicAdd(mine + (p * kBins + ((uint32_t)(k[j] >> s) & (kBins - 1))) * 32, 1u);
+      }
+    }
+  }
+  const uint64_t stride = (uint64_t)gridDim.x * kHistLaneThreads;
+  for (uint64_t i = chunks * KPW + (uint64_t)blockIdx.x * kHistLaneThreads + threadIdx.x; i < n;
+       i += stride) {
+    const K u = enc_bits<K, ENC>(__ldcs(keys + i));
+#pragma unroll
+    for (int p = 0; p < PASSES; ++p)
+      atomicAdd(mine + (p * kBins + ((uint32_t)(u >> (p * kRadixBits)) & (kBins - 1))) * 32, 1u);
+  }
+  __syncthreads();
+  // fold the 32 lane copies of each bin (rotated start: no bank conflicts)
+  for (int i = threadIdx.x; i < PASSES * kBins; i += kHistLaneThreads) {
+    uint32_t c = 0;
+#pragma unroll 8
+    for (int l = 0; l < 32; ++l) c += lanes_sh[i * 32 + ((l + (int)lane) & 31)];
+    if (c) atomicAdd(hist + i, c);
+  }
+}
+
 // ---------------------------------------------------------------- plan --
 
 // One block of 256 threads: exclusive digit offsets per pass (in place over
@@ -773,8 +849,21 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
                                                   (uint64_t)sms * 2);
   {
     TimedLaunch timed(ex, MB_KF_RADIX_HISTOGRAM);
-    radix_histogram_kernel<K, ENC, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks),
-                                             kHistThreads, 0, ex->stream>>>(in_k, n, n_dev, hist);
+    if constexpr (PASSES <= 4) {
+      // lane-private bins: one block per SM
+      const size_t hsmem = (size_t)PASSES * kBins * 32 * sizeof(uint32_t);
+      const uint64_t lane_blocks = std::min<uint64_t>(
+          (n + kHistLaneThreads * 16 - 1) / (kHistLaneThreads * 16), (uint64_t)sms);
+      MB_CUDA(cudaFuncSetAttribute(radix_histogram_lanes_kernel<K, ENC, PASSES>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+      radix_histogram_lanes_kernel<K, ENC, PASSES>
+          <<<(unsigned)std::max<uint64_t>(1, lane_blocks), kHistLaneThreads, hsmem, ex->stream>>>(
+              in_k, n, n_dev, hist);
+    } else {
+      radix_histogram_kernel<K, ENC, PASSES><<<(unsigned)std::max<uint64_t>(1, hist_blocks),
+                                               kHistThreads, 0, ex->stream>>>(in_k, n, n_dev,
+                                                                              hist);
+    }
   }
   MB_CUDA(cudaGetLastError());
   radix_plan_kernel<<<1, kBins, 0, ex->stream>>>(hist, PASSES, n, n_dev, plan, in_k, final_k,
