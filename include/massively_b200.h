@@ -466,6 +466,27 @@ int mb_seg_reduce(mb_executor* exec, const mb_src* values, const uint32_t* offse
                   uint64_t segment_count, int op, const void* init, mb_col out);
 /* ForEachSegment(Sort(less)) (massively/src/seg/mod.rs:379-425): stable sort
  * inside every segment, offsets unchanged. */
+/* ForEachSegment(CountIf / FindIf / AdjacentFind / AllOf / AnyOf / NoneOf /
+ * IsSorted / IsSortedUntil) (massively/src/seg/mod.rs:211-245; oracle
+ * verification/oracle/src/seg.rs:171-283): one u32 per segment into `out`.
+ * COUNT_IF counts the items `op` (an IS_* predicate) passes; FIND_IF gives
+ * the first passing local index, ADJACENT_FIND the first i with
+ * x[i] == x[i+1] (`op` = MB_EQUAL), IS_SORTED_UNTIL the first i with
+ * less(x[i], x[i-1]) (`op` = LESS / GREATER / TOTAL_LESS) -- each the
+ * segment's length when there is none; ALL_OF / ANY_OF / NONE_OF / IS_SORTED
+ * give MFlags. */
+enum {
+  MB_SEG_COUNT_IF = 0,
+  MB_SEG_FIND_IF = 1,
+  MB_SEG_ADJACENT_FIND = 2,
+  MB_SEG_IS_SORTED_UNTIL = 3,
+  MB_SEG_ALL_OF = 4,
+  MB_SEG_ANY_OF = 5,
+  MB_SEG_NONE_OF = 6,
+  MB_SEG_IS_SORTED = 7
+};
+int mb_seg_query(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
+                 uint64_t segment_count, int query, int op, mb_col out);
 int mb_seg_sort(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
                 uint64_t segment_count, int less, mb_col out);
 

@@ -87,6 +87,7 @@ def _declare(L: C.CDLL) -> None:
         "mb_lower_bound": (i32, [vp, src, src, i32, col]),
         "mb_unique": (i32, [vp, src, i32, col, pu32, pu32]),
         "mb_scatter_reduce": (i32, [vp, src, i32, src, _P(C.c_int), _P(C.c_uint64), _P(mb_col)]),
+        "mb_seg_query": (i32, [vp, src, vp, u64, i32, i32, col]),
         "mb_find_if": (i32, [vp, src, i32, pu32, pu32]),
         "mb_is_partitioned": (i32, [vp, src, i32, pu32, pu32]),
         "mb_adjacent_find": (i32, [vp, src, i32, pu32, pu32]),

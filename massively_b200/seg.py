@@ -158,6 +158,65 @@ class Sort:
         self.less = O.pred2(less)
 
 
+class _Query:
+    """A per-segment query: one u32 per segment (seg/mod.rs:211-245)."""
+    query = -1
+
+    def __init__(self, op):
+        self.op = op
+
+    def op_id(self) -> int:
+        return O.unary(self.op).id
+
+
+class CountIf(_Query):
+    """Items the predicate passes."""
+    query = 0
+
+
+class FindIf(_Query):
+    """First passing local index, or the segment's length."""
+    query = 1
+
+
+class AdjacentFind(_Query):
+    """First local i with x[i] == x[i+1], or the segment's length."""
+    query = 2
+
+    def __init__(self, equal=O.Equal):
+        super().__init__(equal)
+
+    def op_id(self) -> int:
+        return O.pred2(self.op).id
+
+
+class IsSortedUntil(_Query):
+    """First local i with less(x[i], x[i-1]), or the segment's length."""
+    query = 3
+
+    def __init__(self, less=O.Less):
+        super().__init__(less)
+
+    def op_id(self) -> int:
+        return O.pred2(self.op).id
+
+
+class AllOf(_Query):
+    query = 4
+
+
+class AnyOf(_Query):
+    query = 5
+
+
+class NoneOf(_Query):
+    query = 6
+
+
+class IsSorted(IsSortedUntil):
+    query = 7
+
+
 class ForEachSegment:
     """ForEachSegment(algorithm).run(exec, segments) (seg/mod.rs:159-243).
     Scans and sorts return a SegmentIterator over new values with the same
@@ -195,4 +254,9 @@ class ForEachSegment:
             out = exec.alloc(dt, len(values))
             check(_L().mb_seg_sort(exec.handle, C.byref(s), off, nseg, a.less.id, out.to_col()))
             return SegmentIterator(out, sgm)
+        if isinstance(a, _Query):
+            out = exec.alloc(np.uint32, nseg)
+            check(_L().mb_seg_query(exec.handle, C.byref(s), off, nseg, a.query, a.op_id(),
+                                    out.to_col()))
+            return out
         raise TypeError(f"unsupported segment algorithm {type(a).__name__}")

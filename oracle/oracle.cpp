@@ -488,6 +488,48 @@ template <class T> int scatter_reduce_t(const void* vals, const uint32_t* idx, u
   return 0;
 }
 
+// Per-segment queries: verification/oracle/src/seg.rs:171-283, one u32 per
+// segment (query ids of include/massively_b200.h MB_SEG_*).
+template <class T> int seg_query_t(const void* in, const uint32_t* off, uint64_t nseg, int query,
+                                   int op, uint32_t* out) {
+  const T* x = (const T*)in;
+  for (uint64_t s = 0; s < nseg; ++s) {
+    const T* v = x + off[s];
+    const uint64_t len = off[s + 1] - off[s];
+    uint64_t r = 0;
+    switch (query) {
+      case MB_SEG_COUNT_IF:
+        for (uint64_t i = 0; i < len; ++i) r += apply_flag<T>(op, v[i]) != 0;
+        break;
+      case MB_SEG_FIND_IF:
+        r = len;
+        for (uint64_t i = 0; i < len; ++i) if (apply_flag<T>(op, v[i])) { r = i; break; }
+        break;
+      case MB_SEG_ADJACENT_FIND:
+        r = len;
+        for (uint64_t i = 0; i + 1 < len; ++i) if (v[i] == v[i + 1]) { r = i; break; }
+        break;
+      case MB_SEG_IS_SORTED_UNTIL: case MB_SEG_IS_SORTED:
+        r = len;
+        for (uint64_t i = 1; i < len; ++i) if (apply_pred2<T>(op, v[i], v[i - 1])) { r = i; break; }
+        if (query == MB_SEG_IS_SORTED) r = r == len;
+        break;
+      case MB_SEG_ALL_OF:
+        r = 1;
+        for (uint64_t i = 0; i < len; ++i) if (!apply_flag<T>(op, v[i])) { r = 0; break; }
+        break;
+      case MB_SEG_ANY_OF: case MB_SEG_NONE_OF:
+        r = 0;
+        for (uint64_t i = 0; i < len; ++i) if (apply_flag<T>(op, v[i])) { r = 1; break; }
+        if (query == MB_SEG_NONE_OF) r = !r;
+        break;
+      default: return -1;
+    }
+    out[s] = (uint32_t)r;
+  }
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -655,6 +697,11 @@ int orc_bounds(int dt, const void* src, uint64_t n, const void* vals, uint64_t m
 int orc_scatter_reduce(int dt, const void* vals, const uint32_t* idx, uint64_t n, int op,
                        const void* init, void* out, uint64_t nout) {
   ORC_DISPATCH(dt, scatter_reduce_t, vals, idx, n, op, init, out, nout);
+  return -1;
+}
+int orc_seg_query(int dt, const void* in, const uint32_t* off, uint64_t nseg, int query, int op,
+                  uint32_t* out) {
+  ORC_DISPATCH(dt, seg_query_t, in, off, nseg, query, op, out);
   return -1;
 }
 int64_t orc_find(int kind, int dt, const void* a, uint64_t na, const void* b, uint64_t nb,

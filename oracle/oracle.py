@@ -77,6 +77,7 @@ def _declare(L: C.CDLL) -> None:
         "orc_unique": (i64, [i32, vp, u64, i32, vp]),
         "orc_find": (i64, [i32, i32, vp, u64, vp, u64, i32]),
         "orc_scatter_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp, u64]),
+        "orc_seg_query": (i32, [i32, vp, vp, u64, i32, i32, vp]),
         "orc_arg": (i32, [i32, i32, vp, u64, i32, vp]),
         "orc_seg_scan": (i32, [i32, vp, vp, u64, i32, i32, vp, vp]),
         "orc_seg_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp]),
@@ -619,3 +620,20 @@ def seg_sort(x, offsets, less: str = "less") -> np.ndarray:
     o = np.empty_like(x)
     lib().orc_seg_sort(_dt(x), _p(x), _p(off), off.size - 1, PRED2[less], _p(o))
     return o
+
+
+SEG_QUERIES = {"count_if": 0, "find_if": 1, "adjacent_find": 2, "is_sorted_until": 3,
+               "all_of": 4, "any_of": 5, "none_of": 6, "is_sorted": 7}
+
+
+def seg_query(x, offsets, query: str, op: str) -> np.ndarray:
+    """verification/oracle/src/seg.rs:171-283: one u32 per segment (a count,
+    a local index or the segment's length, or a 0 / 1 flag)."""
+    x, off = _c(x), _c(offsets).astype(np.uint32)
+    nseg = off.size - 1
+    out = np.zeros(max(nseg, 0), np.uint32)
+    opid = PRED2[op] if op in PRED2 else UNARY[op]
+    if nseg > 0 and lib().orc_seg_query(_dt(x), _p(x), _p(off), nseg, SEG_QUERIES[query], opid,
+                                        _p(out)) != 0:
+        raise TypeError(x.dtype)
+    return out

@@ -304,6 +304,23 @@ SCATTER_REDUCE = [
                np.array([10200, 20400], U32)]),
 ]
 
+# Per-segment queries: massively/tests/seg/api.rs.  `query` is the
+# ForEachSegment algorithm, `want` one u32 per segment (flags as 0 / 1).
+SEG_QUERIES = [
+    dict(src="massively/tests/seg/api.rs:718-741", query="all_of", op="is_even",
+         x=np.array([2, 4, 3, 6], U32), offsets=np.array([0, 2, 4], U32),
+         want=np.array([1, 0], U32)),
+    dict(src="massively/tests/seg/api.rs:744-762", query="all_of", op="is_true",
+         x=np.array([7, 3, 0], U32), offsets=np.array([0, 2, 3], U32),
+         want=np.array([1, 0], U32)),
+    dict(src="massively/tests/seg/api.rs:766-805", query="find_if", op="is_even",
+         x=np.array([2, 4, 6, 1, 1, 3, 5, 7, 8, 8], U32),
+         offsets=np.array([0, 0, 3, 6, 7, 10], U32), want=np.array([0, 0, 3, 1, 1], U32)),
+    dict(src="massively/tests/seg/api.rs:807-813", query="adjacent_find", op="equal",
+         x=np.array([2, 4, 6, 1, 1, 3, 5, 7, 8, 8], U32),
+         offsets=np.array([0, 0, 3, 6, 7, 10], U32), want=np.array([0, 3, 0, 1, 1], U32)),
+]
+
 # massively/tests/vector/api/predicate.rs:17-22: count_if over a lazy
 # counting view of four billion items (u32 lengths above i32::MAX).
 COUNT_IF_FOUR_BILLION = dict(src="massively/tests/vector/api/predicate.rs:17-22",

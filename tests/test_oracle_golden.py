@@ -201,6 +201,12 @@ def test_scatter_reduce_known_answers(orc):
     np.testing.assert_array_equal(got, [7, 4])
 
 
+def test_seg_query_known_answers(orc):
+    for case in K.SEG_QUERIES:
+        np.testing.assert_array_equal(orc.seg_query(case["x"], case["offsets"], case["query"],
+                                                    case["op"]), case["want"], err_msg=case["src"])
+
+
 def test_seg_known_answers(orc):
     for case in K.SEG:
         if case["kind"] == "reduce":
