@@ -395,7 +395,9 @@ class SegScanF32(Workload):
         self.n, self.nseg, self.seed, self.mode = n, nseg, seed, mode
         lg = int(np.log2(n))
         self.name = {"scan": f"seg_inclusive_scan_f32_2^{lg}", "reduce": f"seg_reduce_f32_2^{lg}",
-                     "sort": f"seg_sort_u32_2^{lg}"}[mode] + f"_in_2^{int(np.log2(nseg))}_segments"
+                     "sort": f"seg_sort_u32_2^{lg}",
+                     "count_if": f"seg_count_if_f32_2^{lg}"}[mode] + \
+            f"_in_2^{int(np.log2(nseg))}_segments"
         self.metric = "segmented GB/s"
         self.unit = "GB/s"
         self.dtype = "u32" if mode == "sort" else "f32"
@@ -416,6 +418,8 @@ class SegScanF32(Workload):
             self.out = seg.ForEachSegment(seg.InclusiveScan(op.Add)).run(ex, it)
         elif self.mode == "reduce":
             self.out = seg.ForEachSegment(seg.Reduce(op.Add, np.float32(0))).run(ex, it)
+        elif self.mode == "count_if":
+            self.out = seg.ForEachSegment(seg.CountIf(op.IsPositive)).run(ex, it)
         else:
             self.out = seg.ForEachSegment(seg.Sort(op.Less)).run(ex, it)
 
@@ -424,7 +428,7 @@ class SegScanF32(Workload):
 
     def alg_bytes(self):
         offs = (self.nseg + 1) * 4.0
-        if self.mode == "reduce":
+        if self.mode in ("reduce", "count_if"):
             return self.n * 4.0 + self.nseg * 4.0 + offs
         return self.n * 8.0 + offs  # scan; for the sort a one-pass lower bound
 
@@ -602,6 +606,7 @@ WORKLOADS = {
     "seg_scan_f32": lambda: SegScanF32(n=_n(26)),
     "seg_reduce_f32": lambda: SegScanF32(n=_n(26), mode="reduce"),
     "seg_sort_u32": lambda: SegScanF32(n=_n(26), mode="sort"),
+    "seg_count_if_f32": lambda: SegScanF32(n=_n(26), mode="count_if"),
     "group_by": lambda: GroupByC4(n=_n(27)),
     "reduce_u32": lambda: SimpleWorkload("reduce", _n(30)),
     "merge_u32": lambda: SimpleWorkload("merge", _n(28)),
@@ -614,7 +619,7 @@ WORKLOADS = {
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64",
              "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by", "reduce_u32",
              "merge_u32", "gather_u32", "lower_bound_u32", "find_if_u32",
-             "minmax_element_f32", "scatter_reduce_u32"]
+             "minmax_element_f32", "scatter_reduce_u32", "seg_count_if_f32"]
 
 
 # -------------------------------------------------------------- helpers --

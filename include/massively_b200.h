@@ -522,6 +522,36 @@ int mb_tune_get(mb_executor* exec, int family);
 /* Human-readable description of one configuration (static string). */
 const char* mb_tune_describe(int family, int config);
 
+/* ----------------------------------------------------- user operators ---- */
+
+/* massively's operators are user `#[cube]` trait impls (op::ReductionOp,
+ * op::UnaryOp; massively/src/core/op.rs:33-96) compiled into its kernels.
+ * Beyond the built-in ids above, an operator can be given as CUDA C source
+ * and is compiled at run time (NVRTC, sm_100a):
+ *  - mb_user_op_compile: `source` defines `__device__ T name(T a, T b)`
+ *    over the element type `dtype` (T is typedef'd before it); the operator
+ *    is associative (scans) and also commutative (reduce);
+ *  - mb_user_map_compile: `source` defines `__device__ Out name(In x)`.
+ * The handle is valid on every device and is released by
+ * mb_user_op_destroy.  mb_user_op_check only compiles (no device needed) and
+ * reports a compile error with NVRTC's log as the message.  The algorithms
+ * take a plain column of the compiled type: reduce (vector::reduce,
+ * init op fold), inclusive / exclusive scan (vector::inclusive_scan /
+ * exclusive_scan), map (vector::map). */
+typedef struct mb_user_op mb_user_op;
+int mb_user_op_compile(mb_executor* exec, int dtype, const char* source, const char* name,
+                       mb_user_op** out);
+int mb_user_map_compile(mb_executor* exec, int in_dtype, int out_dtype, const char* source,
+                        const char* name, mb_user_op** out);
+int mb_user_op_check(int kind, int dtype, int out_dtype, const char* source, const char* name);
+int mb_user_op_destroy(mb_user_op* op);
+int mb_reduce_user(mb_executor* exec, const mb_src* in, mb_user_op* op, const void* init,
+                   void* result_dev, void* result_host);
+int mb_inclusive_scan_user(mb_executor* exec, const mb_src* in, mb_user_op* op, mb_col out);
+int mb_exclusive_scan_user(mb_executor* exec, const mb_src* in, mb_user_op* op, const void* init,
+                           mb_col out);
+int mb_map_user(mb_executor* exec, const mb_src* in, mb_user_op* op, mb_col out);
+
 /* ------------------------------------------------------- kernel timing ---- */
 
 /* No counterpart in massively (which has no tracing).  While enabled, the

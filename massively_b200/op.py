@@ -72,3 +72,65 @@ def unary(op) -> UnaryOp:
 
 def pred2(op) -> BinaryPredicateOp:
     return PREDICATES2[op] if isinstance(op, str) else op
+
+
+# ---------------------------------------------------------- user operators --
+
+class UserOp:
+    """An operator written as CUDA C source and compiled at run time (NVRTC)
+    -- the counterpart of a user `#[cube]` impl of op::ReductionOp /
+    op::UnaryOp (massively/src/core/op.rs:33-96).
+
+    binary(exec, dtype, source, name): `source` defines
+    `__device__ T name(T a, T b)` (T is the element type); usable with
+    vector.reduce (associative and commutative) and the scans (associative).
+    map(exec, in_dtype, out_dtype, source, name): `source` defines
+    `__device__ Out name(In x)`; usable with vector.map."""
+
+    def __init__(self, handle, kind: int, dtype, out_dtype):
+        self.handle, self.kind = handle, kind
+        self.dtype, self.out_dtype = dtype, out_dtype
+        self.is_predicate = False
+
+    @classmethod
+    def binary(cls, exec, dtype, source: str, name: str) -> "UserOp":
+        import ctypes as C
+        import numpy as np
+        from . import _native as N
+        from .runtime import NP_TO_ID, check
+        h = C.c_void_p()
+        dt = np.dtype(dtype)
+        check(N.lib().mb_user_op_compile(exec.handle, NP_TO_ID[dt], source.encode(),
+                                         name.encode(), C.byref(h)))
+        return cls(h, 0, dt, dt)
+
+    @classmethod
+    def map(cls, exec, in_dtype, out_dtype, source: str, name: str) -> "UserOp":
+        import ctypes as C
+        import numpy as np
+        from . import _native as N
+        from .runtime import NP_TO_ID, check
+        h = C.c_void_p()
+        i, o = np.dtype(in_dtype), np.dtype(out_dtype)
+        check(N.lib().mb_user_map_compile(exec.handle, NP_TO_ID[i], NP_TO_ID[o], source.encode(),
+                                          name.encode(), C.byref(h)))
+        return cls(h, 1, i, o)
+
+    @staticmethod
+    def check_source(kind: int, dtype, out_dtype, source: str, name: str) -> None:
+        """Compiles without loading (no device needed); raises on an error."""
+        import numpy as np
+        from . import _native as N
+        from .runtime import NP_TO_ID, check
+        check(N.lib().mb_user_op_check(kind, NP_TO_ID[np.dtype(dtype)],
+                                       NP_TO_ID[np.dtype(out_dtype)], source.encode(),
+                                       name.encode()))
+
+    def __del__(self):
+        try:
+            from . import _native as N
+            if self.handle:
+                N.lib().mb_user_op_destroy(self.handle)
+                self.handle = None
+        except Exception:  # interpreter shutdown
+            pass

@@ -107,8 +107,25 @@ def copy(exec: Executor, input, output: DeviceVec) -> None:
     check(_L().mb_copy(exec.handle, C.byref(s), output.to_col()))
 
 
+def _plain(exec: Executor, input, dtype) -> DeviceVec:
+    """The input as a plain column of `dtype` (lazy views are materialised)."""
+    if isinstance(input, DeviceVec) and input.dtype == dtype and input.len_dev is None:
+        return input
+    from .lazy import Map as _Map
+    out = exec.alloc(dtype, _len(input))
+    copy(exec, _Map(input, O.Identity, dtype), out)
+    return out
+
+
 def map(exec: Executor, input, unary, dtype=None) -> DeviceVec:  # noqa: A001
-    """vector::map (transform.rs:91-110) for a built-in unary op."""
+    """vector::map (transform.rs:91-110) for a built-in unary op or a
+    compiled user map (op.UserOp.map)."""
+    if isinstance(unary, O.UserOp):
+        _check_owner(exec, input)
+        x = _plain(exec, input, unary.dtype)
+        out = exec.alloc(unary.out_dtype, len(x))
+        check(_L().mb_map_user(exec.handle, C.byref(x.to_src()), unary.handle, out.to_col()))
+        return out
     from .lazy import Map
     v = Map(input, unary, dtype)
     out = exec.alloc(v.dtype, len(v))
@@ -125,8 +142,15 @@ def fill(exec: Executor, value, output: DeviceVec) -> None:
 # ----------------------------------------------------------------- scan --
 
 def inclusive_scan(exec: Executor, input, op) -> DeviceVec:
-    """vector::inclusive_scan (massively/src/api/algorithm/scan.rs:96)."""
+    """vector::inclusive_scan (massively/src/api/algorithm/scan.rs:96); `op`
+    a built-in or a compiled user operator (op.UserOp.binary)."""
     _check_owner(exec, input)
+    if isinstance(op, O.UserOp):
+        x = _plain(exec, input, op.dtype)
+        out = exec.alloc(op.dtype, len(x))
+        check(_L().mb_inclusive_scan_user(exec.handle, C.byref(x.to_src()), op.handle,
+                                          out.to_col()))
+        return out
     keep = []
     n = _len(input)
     s = lower(exec, input, keep)
@@ -140,6 +164,13 @@ def inclusive_scan(exec: Executor, input, op) -> DeviceVec:
 def exclusive_scan(exec: Executor, input, init, op) -> DeviceVec:
     """vector::exclusive_scan (scan.rs:216)."""
     _check_owner(exec, input)
+    if isinstance(op, O.UserOp):
+        x = _plain(exec, input, op.dtype)
+        out = exec.alloc(op.dtype, len(x))
+        buf = scalar_buffer(init, op.dtype)
+        check(_L().mb_exclusive_scan_user(exec.handle, C.byref(x.to_src()), op.handle, buf,
+                                          out.to_col()))
+        return out
     keep = []
     n = _len(input)
     s = lower(exec, input, keep)
@@ -178,8 +209,16 @@ def adjacent_difference(exec: Executor, input, op) -> DeviceVec:
 
 def reduce(exec: Executor, input, init, op):
     """vector::reduce (massively/src/api/algorithm/reduce.rs:32-50): returns
-    `init op fold(input)` on the host (synchronises)."""
+    `init op fold(input)` on the host (synchronises); `op` a built-in or a
+    compiled user operator (op.UserOp.binary)."""
     _check_owner(exec, input)
+    if isinstance(op, O.UserOp):
+        x = _plain(exec, input, op.dtype)
+        buf = scalar_buffer(init, op.dtype)
+        res = np.zeros(1, dtype=op.dtype)
+        check(_L().mb_reduce_user(exec.handle, C.byref(x.to_src()), op.handle, buf, None,
+                                  res.ctypes.data_as(C.c_void_p)))
+        return res[0]
     keep = []
     _len(input)
     s = lower(exec, input, keep)
