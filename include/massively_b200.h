@@ -487,6 +487,22 @@ enum {
 };
 int mb_seg_query(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
                  uint64_t segment_count, int query, int op, mb_col out);
+/* ForEachSegment(Reverse) and ForEachSegment(AdjacentDifference(op))
+ * (massively/src/seg/mod.rs:177, 191; oracle seg.rs:41-46, 90-107): the
+ * same offsets; `out` holds the transformed values. */
+int mb_seg_reverse(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
+                   uint64_t segment_count, mb_col out);
+int mb_seg_adjacent_difference(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
+                               uint64_t segment_count, int op, mb_col out);
+/* ForEachSegment(Filter(pred) / Take(k) / Unique(equal)) (seg/mod.rs:195-205;
+ * oracle seg.rs:109-153): a stable subsequence of every segment.  `kind` 0 =
+ * filter (`param` an IS_* predicate), 1 = take (`param` = k), 2 = unique
+ * (`param` = MB_EQUAL).  Writes the kept values to `out` (capacity: the input
+ * length) and the new offsets (segment_count + 1 entries) to new_offsets;
+ * the kept count goes to count_dev and / or count_host. */
+int mb_seg_keep(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
+                uint64_t segment_count, int kind, int param, mb_col out, uint32_t* new_offsets,
+                uint32_t* count_dev, uint32_t* count_host);
 int mb_seg_sort(mb_executor* exec, const mb_src* values, const uint32_t* offsets,
                 uint64_t segment_count, int less, mb_col out);
 

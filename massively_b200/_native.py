@@ -88,6 +88,9 @@ def _declare(L: C.CDLL) -> None:
         "mb_unique": (i32, [vp, src, i32, col, pu32, pu32]),
         "mb_scatter_reduce": (i32, [vp, src, i32, src, _P(C.c_int), _P(C.c_uint64), _P(mb_col)]),
         "mb_seg_query": (i32, [vp, src, vp, u64, i32, i32, col]),
+        "mb_seg_reverse": (i32, [vp, src, vp, u64, col]),
+        "mb_seg_adjacent_difference": (i32, [vp, src, vp, u64, i32, col]),
+        "mb_seg_keep": (i32, [vp, src, vp, u64, i32, i32, col, vp, pu32, pu32]),
         "mb_user_op_compile": (i32, [vp, i32, C.c_char_p, C.c_char_p, _P(vp)]),
         "mb_user_map_compile": (i32, [vp, i32, i32, C.c_char_p, C.c_char_p, _P(vp)]),
         "mb_user_op_check": (i32, [i32, i32, i32, C.c_char_p, C.c_char_p]),

@@ -217,6 +217,66 @@ class IsSorted(IsSortedUntil):
     query = 7
 
 
+class Map:
+    """Map(unary): the same segments over mapped values (seg/mod.rs:165)."""
+
+    def __init__(self, unary, dtype=None):
+        self.unary, self.dtype = unary, dtype
+
+
+class Reverse:
+    """Every segment reversed (seg/mod.rs:177)."""
+
+
+class AdjacentDifference:
+    """First item kept, then op(x[i-1], x[i]) inside each segment
+    (seg/mod.rs:191)."""
+
+    def __init__(self, op):
+        self.op = O.reduction(op)
+
+
+class _Keep:
+    kind = -1
+
+    def param(self) -> int:
+        raise NotImplementedError
+
+
+class Filter(_Keep):
+    """The items the predicate passes, per segment (seg/mod.rs:199)."""
+    kind = 0
+
+    def __init__(self, pred):
+        self.pred = O.unary(pred)
+
+    def param(self) -> int:
+        return self.pred.id
+
+
+class Take(_Keep):
+    """The first k items of every segment (seg/mod.rs:203)."""
+    kind = 1
+
+    def __init__(self, count: int):
+        self.count = int(count)
+
+    def param(self) -> int:
+        return self.count
+
+
+class Unique(_Keep):
+    """The first item of every run of equal items, per segment
+    (seg/mod.rs:195)."""
+    kind = 2
+
+    def __init__(self, equal=O.Equal):
+        self.equal = O.pred2(equal)
+
+    def param(self) -> int:
+        return self.equal.id
+
+
 class ForEachSegment:
     """ForEachSegment(algorithm).run(exec, segments) (seg/mod.rs:159-243).
     Scans and sorts return a SegmentIterator over new values with the same
@@ -254,6 +314,25 @@ class ForEachSegment:
             out = exec.alloc(dt, len(values))
             check(_L().mb_seg_sort(exec.handle, C.byref(s), off, nseg, a.less.id, out.to_col()))
             return SegmentIterator(out, sgm)
+        if isinstance(a, Map):
+            from . import vector
+            return SegmentIterator(vector.map(exec, values, a.unary, a.dtype), sgm)
+        if isinstance(a, (Reverse, AdjacentDifference)):
+            out = exec.alloc(dt, len(values))
+            if isinstance(a, Reverse):
+                check(_L().mb_seg_reverse(exec.handle, C.byref(s), off, nseg, out.to_col()))
+            else:
+                check(_L().mb_seg_adjacent_difference(exec.handle, C.byref(s), off, nseg,
+                                                      a.op.id, out.to_col()))
+            return SegmentIterator(out, sgm)
+        if isinstance(a, _Keep):
+            out = exec.alloc(dt, len(values))
+            new_off = exec.alloc(U32, nseg + 1)
+            cnt = C.c_uint32(0)
+            check(_L().mb_seg_keep(exec.handle, C.byref(s), off, nseg, a.kind, a.param(),
+                                   out.to_col(), C.c_void_p(new_off.data_ptr()), None,
+                                   C.byref(cnt)))
+            return SegmentIterator(out.slice(0, cnt.value), Segmentation(new_off, cnt.value))
         if isinstance(a, _Query):
             out = exec.alloc(np.uint32, nseg)
             check(_L().mb_seg_query(exec.handle, C.byref(s), off, nseg, a.query, a.op_id(),

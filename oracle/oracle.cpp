@@ -530,6 +530,35 @@ template <class T> int seg_query_t(const void* in, const uint32_t* off, uint64_t
   return 0;
 }
 
+// Per-segment transforms: verification/oracle/src/seg.rs:41-46 (reverse),
+// 90-107 (adjacent_difference), 109-129 (unique: compared with the last
+// kept item), 131-146 (filter), 148-153 (take).  kind: 0 filter, 1 take,
+// 2 unique, 3 reverse, 4 adjacent_difference.  Writes values to `out` and
+// the new offsets (nseg + 1) to `new_off`; returns the value count.
+template <class T> int64_t seg_transform_t(const void* in, const uint32_t* off, uint64_t nseg,
+                                           int kind, int param, void* out, uint32_t* new_off) {
+  const T* x = (const T*)in;
+  T* o = (T*)out;
+  uint64_t w = 0;
+  new_off[0] = 0;
+  for (uint64_t s = 0; s < nseg; ++s) {
+    const T* v = x + off[s];
+    const uint64_t len = off[s + 1] - off[s];
+    const uint64_t start = w;
+    for (uint64_t i = 0; i < len; ++i) {
+      switch (kind) {
+        case 0: if (apply_flag<T>(param, v[i])) o[w++] = v[i]; break;
+        case 1: if (i < (uint64_t)param) o[w++] = v[i]; break;
+        case 2: if (w == start || !(o[w - 1] == v[i])) o[w++] = v[i]; break;
+        case 3: o[w++] = v[len - 1 - i]; break;
+        default: o[w++] = i == 0 ? v[0] : apply_op<T>(param, v[i - 1], v[i]); break;
+      }
+    }
+    new_off[s + 1] = (uint32_t)w;
+  }
+  return (int64_t)w;
+}
+
 }  // namespace
 
 extern "C" {
@@ -702,6 +731,11 @@ int orc_scatter_reduce(int dt, const void* vals, const uint32_t* idx, uint64_t n
 int orc_seg_query(int dt, const void* in, const uint32_t* off, uint64_t nseg, int query, int op,
                   uint32_t* out) {
   ORC_DISPATCH(dt, seg_query_t, in, off, nseg, query, op, out);
+  return -1;
+}
+int64_t orc_seg_transform(int dt, const void* in, const uint32_t* off, uint64_t nseg, int kind,
+                          int param, void* out, uint32_t* new_off) {
+  ORC_DISPATCH(dt, seg_transform_t, in, off, nseg, kind, param, out, new_off);
   return -1;
 }
 int64_t orc_find(int kind, int dt, const void* a, uint64_t na, const void* b, uint64_t nb,

@@ -78,6 +78,7 @@ def _declare(L: C.CDLL) -> None:
         "orc_find": (i64, [i32, i32, vp, u64, vp, u64, i32]),
         "orc_scatter_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp, u64]),
         "orc_seg_query": (i32, [i32, vp, vp, u64, i32, i32, vp]),
+        "orc_seg_transform": (i64, [i32, vp, vp, u64, i32, i32, vp, vp]),
         "orc_arg": (i32, [i32, i32, vp, u64, i32, vp]),
         "orc_seg_scan": (i32, [i32, vp, vp, u64, i32, i32, vp, vp]),
         "orc_seg_reduce": (i32, [i32, vp, vp, u64, i32, vp, vp]),
@@ -637,3 +638,27 @@ def seg_query(x, offsets, query: str, op: str) -> np.ndarray:
                                         _p(out)) != 0:
         raise TypeError(x.dtype)
     return out
+
+
+SEG_TRANSFORMS = {"filter": 0, "take": 1, "unique": 2, "reverse": 3, "adjacent_difference": 4}
+
+
+def seg_transform(x, offsets, kind: str, param=0):
+    """verification/oracle/src/seg.rs:41-153: (values, new offsets).  param:
+    the predicate name (filter), k (take), the operator name
+    (adjacent_difference)."""
+    x, off = _c(x), _c(offsets).astype(np.uint32)
+    nseg = off.size - 1
+    out = np.empty_like(x)
+    new_off = np.zeros(nseg + 1, np.uint32)
+    if kind == "filter":
+        p = UNARY[param]
+    elif kind == "adjacent_difference":
+        p = OPS[param]
+    else:
+        p = int(param)
+    w = lib().orc_seg_transform(_dt(x), _p(x), _p(off), nseg, SEG_TRANSFORMS[kind], p, _p(out),
+                                _p(new_off))
+    if w < 0:
+        raise TypeError(x.dtype)
+    return out[:w], new_off

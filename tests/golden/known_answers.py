@@ -321,6 +321,19 @@ SEG_QUERIES = [
          offsets=np.array([0, 0, 3, 6, 7, 10], U32), want=np.array([0, 3, 0, 1, 1], U32)),
 ]
 
+# ForEachSegment(Take(k)): massively/tests/seg/api.rs:771-797 -- values and
+# new offsets, empty segments included.
+SEG_TAKE = [
+    dict(src="massively/tests/seg/api.rs:771-784", k=2,
+         x=np.array([2, 4, 6, 1, 1, 3, 5, 7, 8, 8], U32),
+         offsets=np.array([0, 0, 3, 6, 7, 10], U32),
+         values=np.array([2, 4, 1, 1, 5, 7, 8], U32), new_offsets=np.array([0, 0, 2, 4, 5, 7], U32)),
+    dict(src="massively/tests/seg/api.rs:786-797", k=0,
+         x=np.array([2, 4, 6, 1, 1, 3, 5, 7, 8, 8], U32),
+         offsets=np.array([0, 0, 3, 6, 7, 10], U32),
+         values=np.array([], U32), new_offsets=np.array([0, 0, 0, 0, 0, 0], U32)),
+]
+
 # massively/tests/vector/api/predicate.rs:17-22: count_if over a lazy
 # counting view of four billion items (u32 lengths above i32::MAX).
 COUNT_IF_FOUR_BILLION = dict(src="massively/tests/vector/api/predicate.rs:17-22",

@@ -207,6 +207,23 @@ def test_seg_query_known_answers(orc):
                                                     case["op"]), case["want"], err_msg=case["src"])
 
 
+def test_seg_take_known_answers(orc):
+    for case in K.SEG_TAKE:
+        v, off = orc.seg_transform(case["x"], case["offsets"], "take", case["k"])
+        np.testing.assert_array_equal(v, case["values"], err_msg=case["src"])
+        np.testing.assert_array_equal(off, case["new_offsets"], err_msg=case["src"])
+    # unique compares with the last kept item; reverse and adjacent_difference
+    x = np.array([1, 1, 2, 2, 2, 3, 9, 9], np.uint32)
+    off = np.array([0, 3, 3, 8], np.uint32)
+    v, o = orc.seg_transform(x, off, "unique")
+    np.testing.assert_array_equal(v, [1, 2, 2, 3, 9])
+    np.testing.assert_array_equal(o, [0, 2, 2, 5])
+    v, _ = orc.seg_transform(x, off, "reverse")
+    np.testing.assert_array_equal(v, [2, 1, 1, 9, 9, 3, 2, 2])
+    v, _ = orc.seg_transform(x.astype(np.int32), off, "adjacent_difference", "add")
+    np.testing.assert_array_equal(v, [1, 2, 3, 2, 4, 5, 12, 18])
+
+
 def test_seg_known_answers(orc):
     for case in K.SEG:
         if case["kind"] == "reduce":
