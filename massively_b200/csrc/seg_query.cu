@@ -6,9 +6,10 @@
 // a count, a local index (the segment's length when nothing qualifies) or an
 // MFlag.
 //
-// One warp per segment walks it 128 items at a time (four 32-item rounds
-// loaded together), takes the first qualifying local index from a ballot and
-// stops there; counts add the ballots' population counts.  AllOf is "the
+// CountIf is the segmented reduction (ADD) of the predicate's 0 / 1 flags,
+// read through a lazy map.  The other queries: one warp per segment walks it
+// 128 items at a time (four 32-item rounds loaded together), takes the first
+// qualifying local index from a ballot and stops there.  AllOf is "the
 // first failing item is past the end", AnyOf / NoneOf compare the first
 // passing item with the length, IsSorted compares IsSortedUntil with it.
 // Offsets are canonical (validated when the segmentation was built); reads
@@ -19,6 +20,9 @@
 #include "common.cuh"
 #include "dispatch.cuh"
 #include "lookback.cuh"
+
+extern "C" int mb_seg_reduce(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
+                             uint64_t segment_count, int op, const void* init, mb_col out);
 
 namespace mb {
 namespace {
@@ -166,6 +170,18 @@ int mb_seg_query(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
     default: return set_error(MB_ERR_LAUNCH, "unknown segment query");
   }
   if (segment_count == 0) return MB_OK;
+  if (query == MB_SEG_COUNT_IF && values->map == MB_UN_IDENTITY &&
+      values->vtype == values->dtype && values->kind != MB_SRC_ADJACENT) {
+    // a segmented sum of the predicate's 0 / 1 flags: the tiled segmented
+    // reduction, item-parallel, instead of a warp per segment
+    mb_src flags = *values;
+    flags.map = op;
+    flags.vtype = MB_U32;
+    const uint32_t zero = 0;
+    mb_col o = out;
+    o.dtype = MB_U32;
+    return mb_seg_reduce(ex, &flags, offsets, segment_count, MB_OP_ADD, &zero, o);
+  }
   MB_DISPATCH_CTYPE(ct, seg_query_run, ex, *values, offsets, segment_count, query, op,
                     (uint32_t*)out.data);
   return set_error(MB_ERR_LAUNCH, "unsupported element type");
