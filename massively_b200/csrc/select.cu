@@ -9,7 +9,9 @@
 // column is read once), ranks kept rows with warp ballots (warp-striped
 // items, so ranks follow input order), gets the kept-row count of all
 // earlier tiles by decoupled look-back and writes every column's kept rows
-// to consecutive output positions.  The count of kept rows stays on the
+// to consecutive output positions (on the bulk-copy path a ninth warp runs
+// that look-back while the tile lands and the ballots are taken).  The count
+// of kept rows stays on the
 // device (massively's LogicalExtent::Device, massively/src/core/
 // extent.rs:17-36).  partition writes rejected rows after the kept ones,
 // both stable; its boundary comes from one reduction of the flags first.
@@ -173,8 +175,13 @@ __device__ __forceinline__ uint32_t fused_flag(int map, int dtype, uint32_t x) {
   else return map_to<uint32_t>(map, dtype, x) != 0;
 }
 
+// Barrier among the first `count` threads (ids 1..15; 0 is __syncthreads).
+__device__ __forceinline__ void sel_named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 template <bool FUSED, int PRED>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads + 32)
     select_smem_kernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ stencil,
                        uint32_t* __restrict__ out, uint64_t n, int fused_map, int in_dtype,
                        uint32_t invert, uint32_t* count_dev, uint32_t* counter, DevErr err,
@@ -187,6 +194,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_wcount[kWarps];
   __shared__ uint32_t s_excl;
+  __shared__ uint32_t s_agg;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     const uint32_t t = atomicAdd(counter, 1u);
@@ -205,58 +213,66 @@ __global__ void __launch_bounds__(kThreads)
   const uint64_t tile_base = tile * (uint64_t)kSmemTile;
   if (tile_base >= n) return;
   const bool full = tile_base + kSmemTile <= n;
-  if (full) {
-    if (!mbar_wait(&bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-  } else {
-    for (int i = threadIdx.x; i < kSmemTile; i += kThreads) {
-      const bool ok = tile_base + i < n;
-      buf[i] = ok ? in[tile_base + i] : 0u;
-      if constexpr (!FUSED) buf[kSmemTile + i] = ok ? stencil[tile_base + i] : 0u;
+  // The ninth warp runs the look-back from the start, while the tile lands
+  // and the compute warps take their ballots.
+  uint32_t my_ballot = 0;
+  if (warp == kWarps) {
+    uint32_t excl = 0;
+    if (tile > 0) {
+      const Op<uint32_t, MB_OP_ADD> add{MB_OP_ADD};
+      excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add, err, 0u);
     }
-    __syncthreads();
+    if (lane == 0) s_excl = excl;
+  } else {
+    if (full) {
+      if (!mbar_wait(&bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+    } else {
+      for (int i = threadIdx.x; i < kSmemTile; i += kThreads) {
+        const bool ok = tile_base + i < n;
+        buf[i] = ok ? in[tile_base + i] : 0u;
+        if constexpr (!FUSED) buf[kSmemTile + i] = ok ? stencil[tile_base + i] : 0u;
+      }
+      sel_named_sync(1, kThreads);
+    }
+    const uint32_t* wv = buf + warp * 32 * kSmemItems;
+    const uint32_t* ws = wv + kSmemTile;
+    auto flag = [&](int k) -> bool {
+      if (!full) {
+        const uint64_t i = tile_base + (uint64_t)warp * 32 * kSmemItems + k * 32 + lane;
+        if (i >= n) return false;
+      }
+      uint32_t f;
+      if constexpr (FUSED) f = fused_flag<PRED>(fused_map, in_dtype, wv[k * 32 + lane]);
+      else f = ws[k * 32 + lane] != 0;
+      return (f ^ invert) != 0;
+    };
+    // Each round's ballot is kept by lane k (kSmemItems == 32 rounds), so the
+    // write phase reuses it instead of evaluating the predicate again.
+    static_assert(kSmemItems == 32, "one ballot per lane");
+    uint32_t wcount = 0;
+#pragma unroll 8
+    for (int k = 0; k < kSmemItems; ++k) {
+      const unsigned b = __ballot_sync(kFull, flag(k));
+      if (lane == k) my_ballot = b;
+      wcount += __popc(b);
+    }
+    if (lane == 0) s_wcount[warp] = wcount;
+    sel_named_sync(1, kThreads);
+    if (threadIdx.x == 0) {
+      uint32_t agg = 0;
+      for (int w = 0; w < kWarps; ++w) agg += s_wcount[w];
+      s_agg = agg;
+      st.publish(tile, tile == 0 ? kFlagIncl : kFlagAgg, agg);
+    }
+  }
+  __syncthreads();  // s_excl, s_wcount and s_agg are ready
+  if (warp == kWarps) return;
+  if (threadIdx.x == 0) {
+    const uint32_t excl = s_excl, agg = s_agg;
+    if (tile > 0) st.publish(tile, kFlagIncl, excl + agg);
+    if (tile_base + kSmemTile >= n && count_dev) *count_dev = excl + agg;
   }
   const uint32_t* wv = buf + warp * 32 * kSmemItems;
-  const uint32_t* ws = wv + kSmemTile;
-  auto flag = [&](int k) -> bool {
-    if (!full) {
-      const uint64_t i = tile_base + (uint64_t)warp * 32 * kSmemItems + k * 32 + lane;
-      if (i >= n) return false;
-    }
-    uint32_t f;
-    if constexpr (FUSED) f = fused_flag<PRED>(fused_map, in_dtype, wv[k * 32 + lane]);
-    else f = ws[k * 32 + lane] != 0;
-    return (f ^ invert) != 0;
-  };
-  // Each round's ballot is kept by lane k (kSmemItems == 32 rounds), so the
-  // write phase reuses it instead of evaluating the predicate again.
-  static_assert(kSmemItems == 32, "one ballot per lane");
-  uint32_t wcount = 0, my_ballot = 0;
-#pragma unroll 8
-  for (int k = 0; k < kSmemItems; ++k) {
-    const unsigned b = __ballot_sync(kFull, flag(k));
-    if (lane == k) my_ballot = b;
-    wcount += __popc(b);
-  }
-  if (lane == 0) s_wcount[warp] = wcount;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t c = lane < kWarps ? s_wcount[lane] : 0u;
-    uint32_t agg = __reduce_add_sync(kFull, c);
-    const Op<uint32_t, MB_OP_ADD> add{MB_OP_ADD};
-    uint32_t excl = 0;
-    if (tile == 0) {
-      if (lane == 0) st.publish(0, kFlagIncl, agg);
-    } else {
-      if (lane == 0) st.publish(tile, kFlagAgg, agg);
-      excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add, err, 0u);
-      if (lane == 0) st.publish(tile, kFlagIncl, excl + agg);
-    }
-    if (lane == 0) {
-      s_excl = excl;
-      if (tile_base + kSmemTile >= n && count_dev) *count_dev = excl + agg;
-    }
-  }
-  __syncthreads();
   uint32_t run = s_excl;
   for (int w = 0; w < warp; ++w) run += s_wcount[w];
   const unsigned lt = (1u << lane) - 1u;
@@ -332,7 +348,7 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
       const uint64_t stiles = (n + kSmemTile - 1) / kSmemTile;
       auto launch = [&](auto kern) -> int {
         MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<(unsigned)stiles, kThreads, smem, ex->stream>>>(
+        kern<<<(unsigned)stiles, kThreads + 32, smem, ex->stream>>>(
             (const uint32_t*)in[0].data, (const uint32_t*)stencil->data, (uint32_t*)out[0].data, n,
             stencil->map, in[0].dtype, mode == kRemove ? 1u : 0u, count_dev, p.counter, p.err, st);
         MB_CUDA(cudaGetLastError());
