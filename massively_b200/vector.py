@@ -621,6 +621,17 @@ def _opt(r):
     return None if r is None or r == MINDEX_MAX else int(r)
 
 
+def count(exec: Executor, input) -> int:
+    """vector::count (massively/src/api/algorithm/predicate.rs:53): the
+    logical number of items -- a device length when the input carries one
+    (read back), else its length."""
+    _check_owner(exec, input)
+    c = _columns(input)[0]
+    if isinstance(c, DeviceVec):
+        return c.logical_len()
+    return _len(input)
+
+
 def count_if(exec: Executor, input, pred) -> int:
     """vector::count_if (massively/src/api/algorithm/predicate.rs:63-90): the
     number of items the predicate passes -- a sum reduction of the

@@ -294,3 +294,15 @@ def test_errors(ex):
         vector.mismatch(ex, d, ex.to_device(np.array([1, 2], np.uint32)))
     with pytest.raises(Error):
         vector.min_element(ex, d, op.Equal)
+
+
+def test_count_logical_length(ex):
+    """vector::count (predicate.rs:49-51): the logical item count, device
+    lengths included."""
+    from massively_b200 import lazy, vector
+    assert vector.count(ex, ex.to_device(np.array([1, 2, 3, 4], np.uint32))) == 4
+    x = seeded(np.uint32, 10_001, 3)
+    st = (x % 2).astype(np.uint32)
+    sel = vector.copy_where(ex, ex.to_device(x), ex.to_device(st))
+    assert vector.count(ex, sel) == int(st.sum())
+    assert vector.count(ex, lazy.counting(0).take(77)) == 77
