@@ -385,6 +385,37 @@ def lognormal_offsets(ex, nseg, total, seed, mu=3.0, sigma=1.5):
     return np.concatenate([[0], np.cumsum(base)]).astype(np.uint32)
 
 
+def zipf_keys(ex, n, nkeys, seed, s=1.1):
+    """u32 keys Zipf(s) over `nkeys` distinct keys: rank r in [0, nkeys)
+    from an inverse-CDF table (f64 weights (r+1)^-s, cumulated and scaled to
+    2^32) over the full-range uniform_u32 stream of `seed`, then spread over
+    the 32-bit space as rank * 2654435761 mod 2^32 (a bijection)."""
+    import torch
+    ranks = np.arange(1, nkeys + 1, dtype=np.float64)
+    cdf = np.cumsum(ranks ** -s)
+    cdf_u32 = np.minimum(np.floor(cdf / cdf[-1] * 2.0 ** 32), 2.0 ** 32 - 1).astype(np.int64)
+    u = device_uniform_u32(ex, 0, 0xFFFFFFFF, seed, n).tensor.view(torch.int32)
+    u = u.to(torch.int64) & 0xFFFFFFFF
+    table = torch.from_numpy(cdf_u32).to(u.device)
+    rank = torch.searchsorted(table, u, right=True).clamp_(max=nkeys - 1)
+    keys = ex.alloc(np.uint32, n)
+    keys.tensor.view(torch.int32).copy_((rank.to(torch.int64) * 2654435761 & 0xFFFFFFFF)
+                                        .to(torch.int32))
+    return keys
+
+
+def bernoulli_flags(ex, n, p, seed):
+    """u32 flags: 1 where the full-range uniform_u32 stream of `seed` is
+    below floor(p * 2^32), else 0."""
+    import torch
+    fl = device_uniform_u32(ex, 0, 0xFFFFFFFF, seed, n)
+    flag = ex.alloc(np.uint32, n)
+    flag.tensor.view(torch.int32).copy_(
+        ((fl.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF)
+         < int(p * 2 ** 32)).to(torch.int32))
+    return flag
+
+
 class SegScanF32(Workload):
     """ForEachSegment(InclusiveScan(add)) of 2^26 f32 N(0,1) in 2^20 segments
     with lognormal(3, 1.5) lengths; bytes n * (4 + 4) + (S + 1) * 4."""
@@ -458,24 +489,10 @@ class GroupByC4(Workload):
         import torch
 
         from massively_b200 import pipeline
-        ranks = np.arange(1, self.nkeys + 1, dtype=np.float64)
-        cdf = np.cumsum(ranks ** -1.1)
-        cdf_u32 = np.minimum(np.floor(cdf / cdf[-1] * 2.0 ** 32), 2.0 ** 32 - 1).astype(np.int64)
-        u = device_uniform_u32(ex, 0, 0xFFFFFFFF, self.seed, self.n).tensor.view(torch.int32)
-        u = u.to(torch.int64) & 0xFFFFFFFF
-        table = torch.from_numpy(cdf_u32).to(u.device)
-        rank = torch.searchsorted(table, u, right=True).clamp_(max=self.nkeys - 1)
-        self.keys = ex.alloc(np.uint32, self.n)
-        self.keys.tensor.view(torch.int32).copy_((rank.to(torch.int64) * 2654435761 & 0xFFFFFFFF)
-                                                 .to(torch.int32))
-        del u, rank, table
+        self.keys = zipf_keys(ex, self.n, self.nkeys, self.seed)
+        torch.cuda.empty_cache()
         self.values = ex.to_device(host_normal_f32(ex, self.seed + 1, self.n))
-        fl = device_uniform_u32(ex, 0, 0xFFFFFFFF, self.seed + 2, self.n)
-        self.flag = ex.alloc(np.uint32, self.n)
-        self.flag.tensor.view(torch.int32).copy_(
-            ((fl.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF)
-             < int(0.3 * 2 ** 32)).to(torch.int32))
-        del fl
+        self.flag = bernoulli_flags(ex, self.n, 0.3, self.seed + 2)
         other = device_uniform_u32(ex, 0, 0xFFFFFFFF, self.seed + 3, 1 << 20)
         from massively_b200 import vector
         self.other = vector.sort(ex, other)
@@ -511,7 +528,9 @@ class SimpleWorkload(Workload):
     gather through a random permutation (n * 12: indices, the values they
     pick, the output), find_if with no passing item (a full scan, n * 4),
     minmax_element over f32 normals (n * 4) and scatter_reduce of u32 adds
-    into 2^20 counters (n * 8 + 2^20 * 8)."""
+    into 2^20 counters (n * 8 + 2^20 * 8); set_intersection / set_union of two
+    sorted lists of n / 2 u32 uniform over [0, 2^27) ((l + r) * 4 in + the
+    kept items * 4 out)."""
 
     kernel = "single call"
 
@@ -523,7 +542,9 @@ class SimpleWorkload(Workload):
                      "lower_bound": f"lower_bound_u32_2^{lg}_in_2^24",
                      "find_if": f"find_if_u32_2^{lg}_no_hit",
                      "scatter_reduce": f"scatter_reduce_add_u32_2^{lg}_into_2^20",
-                     "minmax": f"minmax_element_f32_2^{lg}"}[kind]
+                     "minmax": f"minmax_element_f32_2^{lg}",
+                     "set_intersection": f"set_intersection_u32_2x2^{lg - 1}",
+                     "set_union": f"set_union_u32_2x2^{lg - 1}"}[kind]
         self.metric = f"{kind} GB/s"
         self.unit = "GB/s"
         self.dtype = "f32" if kind == "minmax" else "u32"
@@ -536,6 +557,12 @@ class SimpleWorkload(Workload):
             h = self.n // 2
             self.a = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 9, h))
             self.b = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 10, h))
+        elif self.kind in ("set_intersection", "set_union"):
+            h = self.n // 2
+            self.a = vector.sort(ex, device_uniform_u32(ex, 0, (1 << 27) - 1, 19, h))
+            self.b = vector.sort(ex, device_uniform_u32(ex, 0, (1 << 27) - 1, 20, h))
+            fn = vector.set_intersection if self.kind == "set_intersection" else vector.set_union
+            self.kept = fn(ex, self.a, self.b).logical_len()
         elif self.kind == "lower_bound":
             self.src = vector.sort(ex, device_uniform_u32(ex, 0, 0xFFFFFFFF, 13, 1 << 24))
             self.x = device_uniform_u32(ex, 0, 0xFFFFFFFF, 14, self.n)
@@ -562,6 +589,10 @@ class SimpleWorkload(Workload):
             self.out = vector.reduce_to_device(ex, self.x, np.uint32(0), op.Add)
         elif self.kind == "merge":
             self.out = vector.merge(ex, self.a, self.b)
+        elif self.kind == "set_intersection":
+            self.out = vector.set_intersection(ex, self.a, self.b)
+        elif self.kind == "set_union":
+            self.out = vector.set_union(ex, self.a, self.b)
         elif self.kind == "lower_bound":
             self.out = vector.lower_bound(ex, self.src, self.x)
         elif self.kind == "scatter_reduce":
@@ -581,6 +612,8 @@ class SimpleWorkload(Workload):
         # stays in L2 after the first probes)
         if self.kind == "scatter_reduce":  # value + index per proposal, 2^20 counters r+w
             return 8.0 * self.n + 8.0 * (1 << 20)
+        if self.kind in ("set_intersection", "set_union"):
+            return 4.0 * self.n + 4.0 * self.kept
         return {"reduce": 4.0, "merge": 8.0, "gather": 12.0, "lower_bound": 8.0, "find_if": 4.0,
                 "minmax": 4.0}[self.kind] * self.n
 
@@ -615,11 +648,14 @@ WORKLOADS = {
     "find_if_u32": lambda: SimpleWorkload("find_if", _n(28)),
     "scatter_reduce_u32": lambda: SimpleWorkload("scatter_reduce", _n(28)),
     "minmax_element_f32": lambda: SimpleWorkload("minmax", _n(28)),
+    "set_intersection_u32": lambda: SimpleWorkload("set_intersection", _n(28)),
+    "set_union_u32": lambda: SimpleWorkload("set_union", _n(28)),
 }
 SECONDARY = ["scan_u32", "scan_f32", "copy_where_u32", "sort_pairs_u32_16bit", "sort_u64",
              "seg_scan_f32", "seg_reduce_f32", "seg_sort_u32", "group_by", "reduce_u32",
              "merge_u32", "gather_u32", "lower_bound_u32", "find_if_u32",
-             "minmax_element_f32", "scatter_reduce_u32", "seg_count_if_f32"]
+             "minmax_element_f32", "scatter_reduce_u32", "seg_count_if_f32",
+             "set_intersection_u32", "set_union_u32"]
 
 
 # -------------------------------------------------------------- helpers --

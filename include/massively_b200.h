@@ -211,6 +211,21 @@ int mb_pool_stats(mb_executor* exec, uint64_t* used, uint64_t* reserved);
 int mb_copy(mb_executor* exec, const mb_src* in, mb_col out);
 /* vector::fill (massively/src/api/algorithm/selection.rs:321). */
 int mb_fill(mb_executor* exec, const void* value, mb_col out);
+/* vector::replace_where (massively/src/api/algorithm/selection.rs:363; core
+ * massively/src/core/selection.rs:471-513): out[c][i] = values[c] wherever
+ * stencil[i] != 0, for each of the `ncols` (1..12) output columns; other
+ * items keep their value.  `values` holds one 8-byte slot per column (value
+ * bits in the low bytes).  LENGTH_MISMATCH{stencil, output} when the lengths
+ * differ. */
+int mb_replace_where(mb_executor* exec, const uint64_t* values, const mb_src* stencil,
+                     const mb_col* out, int ncols);
+/* vector::transform_where (selection.rs:436; core selection.rs:515-595):
+ * out[c][i] = in[c][i] wherever stencil[i] != 0 -- the operator is the
+ * input view's `map` (mb_unary), converted to the output's element type --
+ * other items keep their value.  LENGTH_MISMATCH{input, stencil} and
+ * {input, output} as in massively. */
+int mb_transform_where(mb_executor* exec, const mb_src* in, int ncols, const mb_src* stencil,
+                       const mb_col* out);
 
 /* ------------------------------------------------------------- scan ------ */
 
@@ -531,7 +546,13 @@ int mb_graph_destroy(mb_graph* graph);
 /* Selects the kernel configuration (tile shape) used by an algorithm family
  * for later calls on `exec`; -1 restores the built-in default.  `family` is
  * one of the MB_TUNE_* ids; `config` is below mb_tune_config_count(family). */
-enum { MB_TUNE_SCAN = 0, MB_TUNE_RADIX = 1, MB_TUNE_REDUCE = 2, MB_TUNE_SELECT = 3 };
+enum {
+  MB_TUNE_SCAN = 0,
+  MB_TUNE_RADIX = 1,
+  MB_TUNE_REDUCE = 2,
+  MB_TUNE_SELECT = 3,
+  MB_TUNE_SEG = 4 /* ForEachSegment(Reduce): tile-local folds or a carried look-back */
+};
 int mb_tune_config_count(int family);
 int mb_tune_set(mb_executor* exec, int family, int config);
 int mb_tune_get(mb_executor* exec, int family);
@@ -586,6 +607,18 @@ enum {
 };
 int mb_kernel_timing(mb_executor* exec, int enable);
 int mb_kernel_timing_read(mb_executor* exec, int family, uint64_t* launches, double* total_ms);
+
+/* ------------------------------------------------ failure detection ---- */
+
+/* No counterpart in massively.  Enqueues one of the library's own bounded
+ * waits against a condition that never comes, to show that it ends: kind 0
+ * runs the radix digit look-back of four tiles whose first predecessor never
+ * publishes; kind 1 waits on an mbarrier for bulk-copy bytes that no copy
+ * delivers.  Each wait gives up after the 2 s spin limit, records the
+ * failure and returns (no copy is in flight, the context stays usable); the
+ * next mb_sync reports MB_ERR_LAUNCH ("decoupled look-back wait exceeded its
+ * limit") and clears it. */
+int mb_check_bounded_waits(mb_executor* exec, int kind);
 
 #ifdef __cplusplus
 } /* extern "C" */

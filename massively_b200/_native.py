@@ -65,6 +65,9 @@ def _declare(L: C.CDLL) -> None:
         "mb_pool_stats": (i32, [vp, _P(u64), _P(u64)]),
         "mb_copy": (i32, [vp, src, col]),
         "mb_fill": (i32, [vp, vp, col]),
+        "mb_replace_where": (i32, [vp, _P(u64), src, pcol, i32]),
+        "mb_check_bounded_waits": (i32, [vp, i32]),
+        "mb_transform_where": (i32, [vp, src, i32, src, pcol]),
         "mb_inclusive_scan": (i32, [vp, src, i32, col]),
         "mb_inclusive_scan_noalloc": (i32, [vp, src, i32, col]),
         "mb_exclusive_scan": (i32, [vp, src, i32, vp, col]),

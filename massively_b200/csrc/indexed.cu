@@ -105,6 +105,56 @@ __global__ void __launch_bounds__(kThreads) fill_kernel(void* out, int size, uin
   }
 }
 
+// replace_where: out[i] = value where stencil[i] != 0 (massively's
+// ReplaceWhereOperation, core/selection.rs:471-513: a gather of the value
+// into the selected indices).  Items past the stencil's logical length (a
+// device count) are left alone.
+__global__ void __launch_bounds__(kThreads) replace_where_kernel(void* out, int size,
+                                                                 uint64_t bits, Src stencil,
+                                                                 uint64_t n) {
+  uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x;
+  const uint64_t step = (uint64_t)gridDim.x * kThreads;
+  const uint64_t lim = src_len(stencil) < n ? src_len(stencil) : n;
+  for (; i < lim; i += step) {
+    if (src_load<uint32_t>(stencil, i) == 0) continue;
+    switch (size) {
+      case 1: ((uint8_t*)out)[i] = (uint8_t)bits; break;
+      case 2: ((uint16_t*)out)[i] = (uint16_t)bits; break;
+      case 4: ((uint32_t*)out)[i] = (uint32_t)bits; break;
+      default: ((uint64_t*)out)[i] = bits; break;
+    }
+  }
+}
+
+// transform_where: out[i] = view[i] (the view's map is the operator) where
+// stencil[i] != 0 (massively's TransformWhereInput, core/selection.rs:
+// 515-578); T = the output's compute type.
+template <class T>
+__global__ void __launch_bounds__(kThreads) transform_where_kernel(Src in, Src stencil, void* out,
+                                                                   int out_dtype, uint64_t n) {
+  uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x;
+  const uint64_t step = (uint64_t)gridDim.x * kThreads;
+  uint64_t lim = src_len(stencil) < n ? src_len(stencil) : n;
+  if (src_len(in) < lim) lim = src_len(in);
+  for (; i < lim; i += step)
+    if (src_load<uint32_t>(stencil, i) != 0) st_cast<T>(out_dtype, out, i, src_load<T>(in, i));
+}
+
+template <class T>
+int transform_where_run(mb_executor* ex, const mb_src& in, const mb_src& stencil,
+                        const mb_col& out) {
+  transform_where_kernel<T><<<stride_grid(in.len), kThreads, 0, ex->stream>>>(
+      to_src(in), to_src(stencil), out.data, out.dtype, in.len);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int transform_where_col(mb_executor* ex, const mb_src& in, const mb_src& stencil,
+                        const mb_col& out) {
+  MB_DISPATCH_CTYPE(compute_type(out.dtype), transform_where_run, ex, in, stencil, out);
+  return set_error(MB_ERR_LAUNCH, "unsupported element type");
+}
+
 // gather: out[i] = values[idx[i]] where stencil (if any) is set.  Rows of
 // `size` bytes move as raw bits (no conversion), like massively's copy.
 template <int SIZE>
@@ -336,6 +386,49 @@ int mb_fill(mb_executor* ex, const void* value, mb_col out) {
   fill_kernel<<<stride_grid(out.len), kThreads, 0, ex->stream>>>(
       out.data, (int)dtype_size(out.dtype), bits, out.len);
   MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int mb_replace_where(mb_executor* ex, const uint64_t* values, const mb_src* stencil,
+                     const mb_col* out, int ncols) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, stencil, "stencil"));
+  if (!out || !values || ncols < 1 || ncols > 12)
+    return set_error(MB_ERR_LAUNCH, "replace_where takes 1 to 12 output columns and values");
+  for (int c = 0; c < ncols; ++c) {
+    MB_TRY(check_col(ex, out[c], "output"));
+    if (stencil->len != out[c].len)
+      return set_error(MB_ERR_LENGTH_MISMATCH, "stencil and output lengths differ", stencil->len,
+                       out[c].len);
+  }
+  if (stencil->len == 0) return MB_OK;
+  const Src st = to_src(*stencil);
+  for (int c = 0; c < ncols; ++c) {
+    replace_where_kernel<<<stride_grid(out[c].len), kThreads, 0, ex->stream>>>(
+        out[c].data, (int)dtype_size(out[c].dtype), values[c], st, out[c].len);
+    MB_CUDA(cudaGetLastError());
+  }
+  return MB_OK;
+}
+
+int mb_transform_where(mb_executor* ex, const mb_src* in, int ncols, const mb_src* stencil,
+                       const mb_col* out) {
+  MB_TRY(check_exec(ex));
+  MB_TRY(check_src(ex, stencil, "stencil"));
+  if (!in || !out || ncols < 1 || ncols > 12)
+    return set_error(MB_ERR_LAUNCH, "transform_where takes 1 to 12 columns");
+  for (int c = 0; c < ncols; ++c) {
+    MB_TRY(check_src(ex, &in[c], "input"));
+    MB_TRY(check_col(ex, out[c], "output"));
+    if (in[c].len != stencil->len)
+      return set_error(MB_ERR_LENGTH_MISMATCH, "input and stencil lengths differ", in[c].len,
+                       stencil->len);
+    if (in[c].len != out[c].len)
+      return set_error(MB_ERR_LENGTH_MISMATCH, "input and output lengths differ", in[c].len,
+                       out[c].len);
+  }
+  if (stencil->len == 0) return MB_OK;
+  for (int c = 0; c < ncols; ++c) MB_TRY(transform_where_col(ex, in[c], *stencil, out[c]));
   return MB_OK;
 }
 

@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "dispatch.cuh"
+#include "lookback.cuh"
 
 namespace mb {
 
@@ -174,48 +175,306 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Occurrence-rank flags of `own` against `other` (set.rs:18-46 rules).
-// mode 1 (keep if rank < count in other): intersection;
-// mode 2 (keep if rank >= count in other): difference and union extras.
-template <class T>
+// ------------------------------------------------------ set operations --
+//
+// One pass over the stable merge M of the two inputs (ties: left first).
+// Equivalent items (neither less than the other) form one run of M: its
+// left copies, then its right copies.  With rs / re the run's first and
+// one-past-last merged positions and lr the position of its first right
+// copy (cl = lr - rs left copies, cr = re - lr right copies), massively's
+// multiset rule (core/set.rs:18-46; the two-pointer walk of its oracle,
+// verification/oracle/src/vector.rs:595-664) keeps, for the item at p:
+//   intersection: a left copy with p - rs <  cr;
+//   difference:   a left copy with p - rs >= cr;
+//   union:        every left copy, and a right copy with p - lr >= cl.
+// A tile of M (its merge-path split) merges its two slices in shared
+// memory, finds every position's run with block-wide scans of the run heads
+// and of the left / right positions, and takes the runs that cross its
+// edges from the run of each boundary's item (four binary searches per
+// boundary, for all boundaries at once before the tile kernel).  It counts
+// the kept items, gets the count of all earlier tiles by a decoupled
+// look-back, and writes the kept items in order; the total stays on the
+// device.  The inputs must be sorted under a strict weak order (no NaN
+// under LESS / GREATER; TOTAL_LESS orders every float).
+
+struct SetRun {
+  uint32_t lbl, ubl, lbr, ubr;  // the run's bounds in the left and in the right input
+};
+
+template <class T, int LESS>
+__device__ __forceinline__ bool equiv_ct(T a, T b) {
+  return !cmp_ct<T, LESS>(a, b) && !cmp_ct<T, LESS>(b, a);
+}
+
+// First index in [0, n) whose item is not less than v (UPPER: that v is
+// less than).
+template <class T, int LESS, bool PLAIN, bool UPPER>
+__device__ uint64_t bound_of(const Src& s, uint64_t n, T v) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    const T x = merge_load<T, PLAIN>(s, mid);
+    const bool before = UPPER ? !cmp_ct<T, LESS>(v, x) : cmp_ct<T, LESS>(x, v);
+    if (before) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per tile boundary b: the merge-path split, the item at merged position
+// b * kTile and the bounds of its run in both inputs.
+template <class T, int LESS, bool PLAIN>
 __global__ void __launch_bounds__(kThreads)
-    set_flags_kernel(Src own, Src other, int less, int mode, uint32_t* flags) {
-  const uint64_t n = src_len(own), m = src_len(other);
-  for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * kThreads) {
-    const T v = src_load<T>(own, i);
-    // first position in own whose element is not less than v
-    uint64_t lo = 0, hi = i;
-    while (lo < hi) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (cmp_less<T>(less, src_load<T>(own, mid), v)) lo = mid + 1;
-      else hi = mid;
-    }
-    const uint64_t rank = i - lo;
-    uint64_t a = 0, b = m;
-    while (a < b) {
-      const uint64_t mid = (a + b) >> 1;
-      if (cmp_less<T>(less, src_load<T>(other, mid), v)) a = mid + 1;
-      else b = mid;
-    }
-    uint64_t c = a, e = m;
-    while (c < e) {
-      const uint64_t mid = (c + e) >> 1;
-      if (!cmp_less<T>(less, v, src_load<T>(other, mid))) c = mid + 1;
-      else e = mid;
-    }
-    const uint64_t cnt = c - a;
-    flags[i] = mode == 1 ? (rank < cnt) : (rank >= cnt);
+    set_bounds_kernel(Src L, Src R, uint64_t tiles, uint64_t* __restrict__ splits,
+                      SetRun* __restrict__ runs, T* __restrict__ vals) {
+  const uint64_t nl = src_len(L), nr = src_len(R), n = nl + nr;
+  for (uint64_t b = blockIdx.x * (uint64_t)kThreads + threadIdx.x; b <= tiles;
+       b += (uint64_t)gridDim.x * kThreads) {
+    const uint64_t d = min(b * (uint64_t)kTile, n);
+    const uint64_t i = merge_path<T, LESS, PLAIN>(L, R, nl, nr, d);
+    splits[b] = i;
+    if (d >= n) continue;
+    const uint64_t j = d - i;
+    const bool from_left =
+        i < nl && (j >= nr || !cmp_ct<T, LESS>(merge_load<T, PLAIN>(R, j),
+                                               merge_load<T, PLAIN>(L, i)));
+    const T v = from_left ? merge_load<T, PLAIN>(L, i) : merge_load<T, PLAIN>(R, j);
+    vals[b] = v;
+    SetRun r;
+    r.lbl = (uint32_t)bound_of<T, LESS, PLAIN, false>(L, nl, v);
+    r.ubl = (uint32_t)bound_of<T, LESS, PLAIN, true>(L, nl, v);
+    r.lbr = (uint32_t)bound_of<T, LESS, PLAIN, false>(R, nr, v);
+    r.ubr = (uint32_t)bound_of<T, LESS, PLAIN, true>(R, nr, v);
+    runs[b] = r;
   }
 }
 
-__global__ void add_counts_kernel(const uint32_t* a, uint64_t b, uint32_t* out) {
-  *out = *a + (uint32_t)b;
+constexpr int kNone = 0x7FFFFFFF;
+
+// Exclusive block-wide scans over the threads' chunk summaries: a running
+// maximum of (a, b) from the left, and a running minimum of (c, d) from the
+// right (each thread gets the extremes of the chunks before / after it).
+__device__ __forceinline__ void set_block_scans(int& a, int& b, int& c, int& d, int* s_tmp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int W = kThreads / 32;
+  int ia = a, ib = b, ic = c, id = d;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int oa = __shfl_up_sync(kFull, ia, off), ob = __shfl_up_sync(kFull, ib, off);
+    const int oc = __shfl_down_sync(kFull, ic, off), od = __shfl_down_sync(kFull, id, off);
+    if (lane >= off) { ia = max(ia, oa); ib = max(ib, ob); }
+    if (lane + off < 32) { ic = min(ic, oc); id = min(id, od); }
+  }
+  if (lane == 31) { s_tmp[warp] = ia; s_tmp[W + warp] = ib; }
+  if (lane == 0) { s_tmp[2 * W + warp] = ic; s_tmp[3 * W + warp] = id; }
+  __syncthreads();
+  int ca = -1, cb = -1, cc = kNone, cd = kNone;
+  for (int w = 0; w < warp; ++w) { ca = max(ca, s_tmp[w]); cb = max(cb, s_tmp[W + w]); }
+  for (int w = warp + 1; w < W; ++w) { cc = min(cc, s_tmp[2 * W + w]); cd = min(cd, s_tmp[3 * W + w]); }
+  const int pa = __shfl_up_sync(kFull, ia, 1), pb = __shfl_up_sync(kFull, ib, 1);
+  const int pc = __shfl_down_sync(kFull, ic, 1), pd = __shfl_down_sync(kFull, id, 1);
+  a = lane > 0 ? max(ca, pa) : ca;
+  b = lane > 0 ? max(cb, pb) : cb;
+  c = lane < 31 ? min(cc, pc) : cc;
+  d = lane < 31 ? min(cd, pd) : cd;
 }
 
-unsigned grid_n(uint64_t n) {
-  uint64_t g = (n + kThreads - 1) / kThreads;
-  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 16));
+// MODE: 0 union, 1 intersection, 2 difference.
+template <class T, int LESS, bool PLAIN>
+__global__ void __launch_bounds__(kThreads)
+    set_tile_kernel(int MODE, Src L, Src R, void* out, int out_esize, uint32_t* count_dev,
+                    const uint64_t* __restrict__ splits, const SetRun* __restrict__ runs,
+                    const T* __restrict__ vals, uint32_t* counter, TileState<uint32_t, true> st,
+                    DevErr err) {
+  __shared__ T s_keys[kTile];
+  __shared__ T s_out[kTile];
+  __shared__ uint8_t s_right[kTile];
+  __shared__ int s_tmp[4 * (kThreads / 32)];
+  __shared__ uint32_t s_wcount[kThreads / 32];
+  __shared__ uint32_t s_tile, s_excl;
+  __shared__ uint64_t s_split[2];
+  const uint64_t nl = src_len(L), nr = src_len(R), n = nl + nr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(counter, 1u);
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t d0 = tile * (uint64_t)kTile;
+  if (d0 >= n) return;
+  const uint64_t d1 = min(d0 + (uint64_t)kTile, n);
+  if (tid < 2) s_split[tid] = splits[tile + tid];
+  __syncthreads();
+  const uint64_t i0 = s_split[0], i1 = s_split[1];
+  const uint64_t j0 = d0 - i0, j1 = d1 - i1;
+  const int la = (int)(i1 - i0), lb = (int)(j1 - j0);
+  for (int t = tid; t < la; t += kThreads) s_keys[t] = merge_load<T, PLAIN>(L, i0 + t);
+  for (int t = tid; t < lb; t += kThreads) s_keys[la + t] = merge_load<T, PLAIN>(R, j0 + t);
+  __syncthreads();
+  const int total = la + lb;
+  const int dt = min(tid * kItems, total);
+  {
+    int lo = dt > lb ? dt - lb : 0, hi = dt < la ? dt : la;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (!cmp_ct<T, LESS>(s_keys[la + dt - 1 - mid], s_keys[mid])) lo = mid + 1;
+      else hi = mid;
+    }
+    int a = lo, b = dt - lo;
+    T ka = a < la ? s_keys[a] : T(0);
+    T kb = b < lb ? s_keys[la + b] : T(0);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      if (dt + k >= total) break;
+      const bool take_left = b >= lb || (a < la && !cmp_ct<T, LESS>(kb, ka));
+      s_out[dt + k] = take_left ? ka : kb;
+      s_right[dt + k] = take_left ? 0 : 1;
+      if (take_left) {
+        ++a;
+        ka = a < la ? s_keys[a] : ka;
+      } else {
+        ++b;
+        kb = b < lb ? s_keys[la + b] : kb;
+      }
+    }
+  }
+  __syncthreads();
+
+  // Chunk summaries: last head, last left position (forward); first head,
+  // first right position (backward).  Position 0 is a head of the tile.
+  const int cnt = min(kItems, total - dt);
+  bool head[kItems], right[kItems];
+  int lastH = -1, lastL = -1, firstH = kNone, firstR = kNone;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const int t = dt + k;
+    head[k] = false;
+    right[k] = false;
+    if (k < cnt) {
+      head[k] = t == 0 || !equiv_ct<T, LESS>(s_out[t - 1], s_out[t]);
+      right[k] = s_right[t] != 0;
+      if (head[k]) { lastH = t; if (firstH == kNone) firstH = t; }
+      if (right[k]) { if (firstR == kNone) firstR = t; } else { lastL = t; }
+    }
+  }
+  int eh = lastH, el = lastL, fh = firstH, fr = firstR;
+  set_block_scans(eh, el, fh, fr, s_tmp);
+  // rs / last left (at or before t) forward; re (head after t) / first right
+  // (at or after t) backward -- tile positions.
+  int rs[kItems], ll[kItems], re[kItems], rr[kItems];
+  {
+    int h = eh, l = el;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      if (k < cnt) {
+        if (head[k]) h = dt + k;
+        if (!right[k]) l = dt + k;
+      }
+      rs[k] = h;
+      ll[k] = l;
+    }
+    int nh = fh, nrp = fr;
+#pragma unroll
+    for (int k = kItems - 1; k >= 0; --k) {
+      re[k] = nh;
+      if (k < cnt) {
+        if (right[k]) nrp = dt + k;
+        if (head[k]) nh = dt + k;
+      }
+      rr[k] = nrp;
+    }
+  }
+  // Runs that cross the tile's edges: the first (when it started before
+  // d0) from boundary `tile`, the last (when it goes on past d1) from
+  // boundary `tile + 1`.
+  const SetRun r0 = runs[tile];
+  const uint64_t rs0 = (uint64_t)r0.lbl + r0.lbr;
+  const bool first_open = rs0 < d0;
+  bool last_open = false;
+  SetRun r1{};
+  if (d1 < n) {
+    r1 = runs[tile + 1];
+    last_open = equiv_ct<T, LESS>(s_out[total - 1], vals[tile + 1]);
+  }
+  // Tile position of the last run's head (every thread reads the same).
+  __shared__ int s_last_rs;
+  if (tid == 0) s_last_rs = -1;
+  __syncthreads();
+  if (cnt > 0 && dt + cnt == total) s_last_rs = rs[cnt - 1];
+  __syncthreads();
+  const int last_rs = s_last_rs;
+
+  bool keep[kItems];
+  uint32_t kept = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    keep[k] = false;
+    if (k >= cnt) continue;
+    const uint64_t g = d0 + dt + k;
+    uint64_t grs, glr, gre;
+    const bool use0 = first_open && rs[k] == 0;
+    const bool use1 = !use0 && last_open && rs[k] == last_rs;
+    if (use0 || use1) {
+      const SetRun x = use0 ? r0 : r1;
+      grs = (uint64_t)x.lbl + x.lbr;
+      glr = grs + (x.ubl - x.lbl);
+      gre = (uint64_t)x.ubl + x.ubr;
+    } else {
+      const int e = re[k] == kNone ? total : re[k];
+      int lr;
+      if (!right[k]) lr = min(rr[k] == kNone ? total : rr[k], e);
+      else lr = max(ll[k] + 1, rs[k]);
+      grs = d0 + rs[k];
+      glr = d0 + lr;
+      gre = d0 + e;
+    }
+    bool kp;
+    if (!right[k]) {
+      const uint64_t rank = g - grs, other = gre - glr;
+      kp = MODE == 0 ? true : MODE == 1 ? rank < other : rank >= other;
+    } else {
+      kp = MODE == 0 && (g - glr) >= (glr - grs);
+    }
+    keep[k] = kp;
+    kept += kp ? 1u : 0u;
+  }
+
+  // Output offsets: warp and block prefix of the kept counts, then the
+  // counts of all earlier tiles by the look-back.
+  uint32_t incl = kept;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t o = __shfl_up_sync(kFull, incl, off);
+    if (lane >= off) incl += o;
+  }
+  if (lane == 31) s_wcount[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t c = lane < kThreads / 32 ? s_wcount[lane] : 0u;
+    const uint32_t agg = __reduce_add_sync(kFull, c);
+    const Op<uint32_t, MB_OP_ADD> add{MB_OP_ADD};
+    uint32_t excl = 0;
+    if (tile == 0) {
+      if (lane == 0) st.publish(0, kFlagIncl, agg);
+    } else {
+      if (lane == 0) st.publish(tile, kFlagAgg, agg);
+      excl = lookback_exclusive<uint32_t, Op<uint32_t, MB_OP_ADD>, false>(st, tile, add, err, 0u);
+      if (lane == 0) st.publish(tile, kFlagIncl, excl + agg);
+    }
+    if (lane == 0) {
+      s_excl = excl;
+      if (d1 == n && count_dev) *count_dev = excl + agg;
+    }
+  }
+  __syncthreads();
+  uint32_t pos = s_excl + incl - kept;
+  for (int w = 0; w < warp; ++w) pos += s_wcount[w];
+  const uint64_t cap = MODE == 0 ? n : nl;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (!keep[k]) continue;
+    if (pos < cap) st_raw_pay(out, pos, out_esize, to_bits64(s_out[dt + k]));
+    else raise_device_error(err, MB_DEV_ERR_BOUNDS);  // only after a failed look-back
+    ++pos;
+  }
 }
 
 template <class T, int LESS, bool PLAIN>
@@ -255,14 +514,51 @@ int merge_run(mb_executor* ex, const mb_src& l, const mb_src& r, int less, void*
   }
 }
 
-template <class T>
-int set_flags_run(mb_executor* ex, const mb_src& own, const mb_src& other, int less, int mode,
-                  uint32_t* flags) {
-  if (own.len == 0) return MB_OK;
-  set_flags_kernel<T><<<grid_n(own.len), kThreads, 0, ex->stream>>>(to_src(own), to_src(other),
-                                                                    less, mode, flags);
+// Set operation over n = |l| + |r| > 0 merged items (mode 0 union, 1
+// intersection, 2 difference); the kept count goes to count_dev.
+template <class T, int LESS, bool PLAIN>
+int set_launch(mb_executor* ex, const mb_src& l, const mb_src& r, int mode, const mb_col& out,
+               uint32_t* count_dev) {
+  const uint64_t n = l.len + r.len;
+  const uint64_t tiles = (n + kTile - 1) / kTile;
+  const size_t state_b = TileState<uint32_t, true>::bytes(tiles);
+  const size_t splits_b = ((tiles + 1) * 8 + 255) / 256 * 256;
+  const size_t runs_b = ((tiles + 1) * sizeof(SetRun) + 255) / 256 * 256;
+  const size_t vals_b = ((tiles + 1) * sizeof(T) + 255) / 256 * 256;
+  Scratch scratch;
+  MB_TRY(scratch.alloc(ex, 256 + state_b + splits_b + runs_b + vals_b));
+  char* base = scratch.as<char>();
+  MB_CUDA(cudaMemsetAsync(base, 0, 256 + state_b, ex->stream));
+  uint64_t* splits = (uint64_t*)(base + 256 + state_b);
+  SetRun* runs = (SetRun*)(base + 256 + state_b + splits_b);
+  T* vals = (T*)(base + 256 + state_b + splits_b + runs_b);
+  const uint64_t sblocks = std::min<uint64_t>((tiles + kThreads) / kThreads, 4096);
+  set_bounds_kernel<T, LESS, PLAIN><<<(unsigned)sblocks, kThreads, 0, ex->stream>>>(
+      to_src(l), to_src(r), tiles, splits, runs, vals);
+  MB_CUDA(cudaGetLastError());
+  const DevErr err{ex->status_dev, (uint32_t*)base + 1};
+  set_tile_kernel<T, LESS, PLAIN><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
+      mode, to_src(l), to_src(r), out.data, (int)dtype_size(out.dtype), count_dev, splits, runs,
+      vals,
+      (uint32_t*)base, TileState<uint32_t, true>::make(base + 256, tiles), err);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
+}
+
+template <class T>
+int set_run(mb_executor* ex, const mb_src& l, const mb_src& r, int less, int mode,
+            const mb_col& out, uint32_t* count_dev) {
+  const int ct = DTypeOf<T>::value;
+  const bool plain = src_plain(l, ct) && src_plain(r, ct);
+#define MB_SET_LESS(LESSID)                                                              \
+  return plain ? set_launch<T, LESSID, true>(ex, l, r, mode, out, count_dev)             \
+               : set_launch<T, LESSID, false>(ex, l, r, mode, out, count_dev)
+  switch (less) {
+    case MB_GREATER: MB_SET_LESS(MB_GREATER);
+    case MB_TOTAL_LESS: MB_SET_LESS(MB_TOTAL_LESS);
+    default: MB_SET_LESS(MB_LESS);
+  }
+#undef MB_SET_LESS
 }
 
 int merge_dispatch(mb_executor* ex, const mb_src& l, const mb_src& r, int less, void* out,
@@ -272,10 +568,10 @@ int merge_dispatch(mb_executor* ex, const mb_src& l, const mb_src& r, int less, 
   return set_error(MB_ERR_LAUNCH, "unsupported element type");
 }
 
-int flags_dispatch(mb_executor* ex, const mb_src& own, const mb_src& other, int less, int mode,
-                   uint32_t* flags) {
-  const int ct = compute_type(own.vtype);
-  MB_DISPATCH_CTYPE(ct, set_flags_run, ex, own, other, less, mode, flags);
+int set_dispatch(mb_executor* ex, const mb_src& l, const mb_src& r, int less, int mode,
+                 const mb_col& out, uint32_t* count_dev) {
+  const int ct = compute_type(l.vtype);
+  MB_DISPATCH_CTYPE(ct, set_run, ex, l, r, less, mode, out, count_dev);
   return set_error(MB_ERR_LAUNCH, "unsupported element type");
 }
 
@@ -299,46 +595,16 @@ int set_op(mb_executor* ex, const mb_src* l, const mb_src* r, int less, mb_col o
   if (out.len < need) return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", need, out.len);
   if (dtype_size(out.dtype) != dtype_size(l->vtype))
     return set_error(MB_ERR_LAUNCH, "output element type differs from the input's");
+  MB_TRY(check_len_u32(l->len + r->len));
   Scratch cnt;
   if (!count_dev) {
     MB_TRY(cnt.alloc(ex, 16));
     count_dev = cnt.as<uint32_t>();
   }
-  const mb_src& own = mode == 0 ? *r : *l;
-  const mb_src& other = mode == 0 ? *l : *r;
-  Scratch flags;
-  MB_TRY(flags.alloc(ex, std::max<uint64_t>(16, own.len * 4)));
-  MB_TRY(flags_dispatch(ex, own, other, less, mode == 1 ? 1 : 2, flags.as<uint32_t>()));
-  mb_src st{};
-  st.kind = MB_SRC_COLUMN;
-  st.dtype = st.vtype = MB_U32;
-  st.map = MB_UN_IDENTITY;
-  st.data = flags.ptr;
-  st.len = own.len;
-  if (mode != 0) {
-    MB_TRY(mb_copy_where(ex, l, 1, &st, &out, count_dev, nullptr));
-  } else {
-    // Union: merge left with the right input's extra copies.
-    Scratch extras, ecount;
-    MB_TRY(extras.alloc(ex, std::max<uint64_t>(16, r->len * dtype_size(r->vtype))));
-    MB_TRY(ecount.alloc(ex, 16));
-    mb_col ec{};
-    ec.data = extras.ptr;
-    ec.dtype = r->vtype;
-    ec.len = r->len;
-    MB_TRY(mb_copy_where(ex, r, 1, &st, &ec, ecount.as<uint32_t>(), nullptr));
-    mb_src es{};
-    es.kind = MB_SRC_COLUMN;
-    es.dtype = es.vtype = r->vtype;
-    es.map = MB_UN_IDENTITY;
-    es.data = extras.ptr;
-    es.len = r->len;
-    es.len_dev = ecount.as<uint32_t>();
-    Payload none{};
-    MB_TRY(merge_dispatch(ex, *l, es, less, out.data, out.dtype, none, nullptr));
-    add_counts_kernel<<<1, 1, 0, ex->stream>>>(ecount.as<uint32_t>(), l->len, count_dev);
-    MB_CUDA(cudaGetLastError());
-  }
+  // Zero first: inputs whose device lengths are both 0 launch no tile that
+  // writes the count.
+  MB_CUDA(cudaMemsetAsync(count_dev, 0, 4, ex->stream));
+  if (l->len + r->len > 0) MB_TRY(set_dispatch(ex, *l, *r, less, mode, out, count_dev));
   if (count_host) MB_TRY(read_u32(ex, count_dev, count_host));
   return MB_OK;
 }

@@ -42,7 +42,70 @@ constexpr int kRadixBits = 8;
 constexpr int kBins = 1 << kRadixBits;
 constexpr int kHistThreads = 512;
 constexpr int kHistUnroll = 4;  // 16-byte vectors per lane per chunk
-constexpr uint32_t kCountMask = 0x3FFFFFFFu;  // status: 2 flag bits + 30 count bits
+
+// Look-back status word of one (tile, digit): the flag (none / aggregate /
+// inclusive) in the top two bits, the digit's count below.  32-bit words
+// hold counts below 2^30; a sort of 2^30 items or more uses 64-bit words, so
+// every length up to 2^32 - 1 sorts.
+template <class SW>
+struct DigitStatus {
+  static constexpr int kShift = 8 * (int)sizeof(SW) - 2;
+  static constexpr SW kMask = ((SW)1 << kShift) - 1;
+
+  __device__ __forceinline__ static SW load(const SW* p) {
+    if constexpr (sizeof(SW) == 8) return ld_relaxed_u64(p);
+    else return ld_relaxed_u32(p);
+  }
+  __device__ __forceinline__ static void store(SW* p, uint32_t flag, SW count) {
+    const SW w = ((SW)flag << kShift) | (count & kMask);
+    if constexpr (sizeof(SW) == 8) st_relaxed_u64(p, w);
+    else st_relaxed_u32(p, w);
+  }
+
+  // Publishes digit d's count of `tile` (inclusive for tile 0).
+  __device__ __forceinline__ static void publish(SW* status, uint64_t tile, int d, SW count) {
+    store(status + tile * kBins + d, tile == 0 ? kFlagIncl : kFlagAgg, count);
+  }
+
+  // Decoupled look-back of digit d, eight predecessors per step, bounded:
+  // the count of digit d in all tiles before `tile`; publishes this tile's
+  // inclusive count.  After a wait that ran out it records the failure and
+  // returns the partial sum (never more than the true count).
+  __device__ __forceinline__ static SW lookback(SW* status, uint64_t tile, int d, SW tile_count,
+                                                const DevErr& err) {
+    SW excl = 0;
+    if (tile == 0) return 0;
+    constexpr int kBatch = 8;
+    SpinGuard guard(err.abort);
+    int64_t t = (int64_t)tile - 1;  // next predecessor to account for
+    bool failed = false, done = false;
+    while (!done) {
+      SW w[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j)
+        w[j] = t - j >= 0 ? load(status + (uint64_t)(t - j) * kBins + d)
+                          : ((SW)kFlagIncl << kShift);
+      int used = 0;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        if (done || used < j) break;
+        const uint32_t f = (uint32_t)(w[j] >> kShift);
+        if (f == kFlagNone) break;
+        excl += w[j] & kMask;
+        ++used;
+        if (f == kFlagIncl) done = true;
+      }
+      t -= used;
+      if (!done && used < kBatch && guard.expired()) {
+        failed = true;
+        break;
+      }
+    }
+    if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+    store(status + tile * kBins + d, kFlagIncl, excl + tile_count);
+    return excl;
+  }
+};
 
 // Keys travel as their raw unsigned bits (K = uint32_t / uint64_t) and are
 // never held in floating-point registers; ENC (enc_bits, common.cuh) selects
@@ -299,11 +362,11 @@ struct OnesweepSmem {
   V vals[std::is_same<V, uint8_t>::value ? 1 : TILE];
 };
 
-// V = uint8_t means "keys only".
-template <class K, int ENC, class V, int THREADS, int ITEMS>
+// V = uint8_t means "keys only"; SW the look-back status word (DigitStatus).
+template <class K, int ENC, class V, int THREADS, int ITEMS, class SW>
 __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
     radix_onesweep_kernel(const PassPlan* __restrict__ plan, int pass, uint64_t n,
-                          const uint32_t* __restrict__ digit_offsets, uint32_t* __restrict__ status,
+                          const uint32_t* __restrict__ digit_offsets, SW* __restrict__ status,
                           uint32_t* __restrict__ counter, DevErr err) {
   constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
   using S = OnesweepSmem<K, V, THREADS, ITEMS>;
@@ -385,8 +448,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
       sm.warp_cnt[w][tid] = tile_count;
       tile_count += c;
     }
-    const uint32_t flag = tile == 0 ? kFlagIncl : kFlagAgg;
-    st_relaxed_u32(status + tile * kBins + tid, (flag << 30) | tile_count);
+    DigitStatus<SW>::publish(status, tile, tid, tile_count);
     uint32_t incl = tile_count;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -424,37 +486,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS <= 256 ? 4 : 2))
     }
   }
 
-  // Decoupled look-back, one digit per thread, eight predecessors per step.
+  // Decoupled look-back, one digit per thread.
   if (tid < kBins) {
-    uint32_t excl = 0;
-    if (tile > 0) {
-      constexpr int kBatch = 8;
-      SpinGuard guard(err.abort);
-      int64_t t = (int64_t)tile - 1;  // next predecessor to account for
-      bool failed = false, done = false;
-      while (!done) {
-        uint32_t w[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j)
-          w[j] = t - j >= 0 ? ld_relaxed_u32(status + (uint64_t)(t - j) * kBins + tid)
-                            : (kFlagIncl << 30);
-        int used = 0;
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
-          if (done || used < j) break;
-          const uint32_t f = w[j] >> 30;
-          if (f == kFlagNone) break;
-          excl += w[j] & kCountMask;
-          ++used;
-          if (f == kFlagIncl) done = true;
-        }
-        t -= used;
-        if (!done && used < kBatch && guard.expired()) { failed = true; break; }
-      }
-      if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-      st_relaxed_u32(status + tile * kBins + tid,
-                     (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
-    }
+    const uint32_t excl = (uint32_t)DigitStatus<SW>::lookback(status, tile, tid, tile_count, err);
     sm.delta[tid] = digit_offsets[pass * kBins + tid] + excl - sm.tile_start[tid];
   }
   if constexpr (!KEYS_ONLY) {
@@ -506,6 +540,7 @@ size_t onesweep_smem() {
 // address apply in issue order, which keeps the ranks stable), and
 // broadcasts the old count to its peers.
 
+// NT = 0: peers come from ballots on the digit bits (no mask table).
 template <class K, class V, int THREADS, int ITEMS, int NT>
 struct OnesweepTmaSmem {
   static constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
@@ -513,8 +548,9 @@ struct OnesweepTmaSmem {
   static constexpr int TILE = THREADS * ITEMS;
   K keys[TILE];                       // 16-byte aligned: bulk-copy target
   V vals[KEYS_ONLY ? 16 : TILE];
-  // Slot kBins takes the empty items of a partial tile.
-  uint32_t mask[NT][WARPS][kBins + 1];
+  // Slot kBins takes the empty items of a partial tile.  With NT = 0 the
+  // one-word `mask` array is unused.
+  uint32_t mask[NT <= 0 ? 1 : NT][NT <= 0 ? 1 : WARPS][NT <= 0 ? 1 : kBins + 1];
   uint32_t warp_cnt[WARPS][kBins + 1];
   uint32_t tile_start[kBins];
   uint32_t delta[kBins];
@@ -524,12 +560,12 @@ struct OnesweepTmaSmem {
   uint64_t bar;
 };
 
-template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool P64, bool FULL>
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool P64, bool FULL, class SW>
 __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>& sm,
                                               const uint32_t tile, const uint32_t valid,
                                               const int pass, const uint32_t n,
                                               const uint32_t* __restrict__ digit_offsets,
-                                              uint32_t* __restrict__ status, const DevErr err,
+                                              SW* __restrict__ status, const DevErr err,
                                               K* __restrict__ out_k, V* __restrict__ out_v) {
   using S = OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>;
   constexpr bool KEYS_ONLY = S::KEYS_ONLY;
@@ -545,37 +581,75 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
   const uint32_t below_me = (1u << lane) - 1u;
   const uint32_t me = 1u << lane;
 
-  uint32_t peers[ITEMS];
   uint32_t rd[ITEMS];  // digit << 16, then | rank
+  if constexpr (NT <= 0) {
+    // Peers from one ballot per digit bit: a lane's peers are the lanes
+    // whose every bit agrees with its own.  No shared memory is touched for
+    // them, so the ranking costs no bank conflicts (ALU work instead).  Bit 8
+    // marks the empty items of a partial tile (digit kBins), which then form
+    // a group of their own.  Per round the lowest peer (the leader) adds the
+    // group's size to the warp's digit counter right away; the rounds'
+    // atomics are issued in round order, which keeps the ranks stable.  Each
+    // item keeps, packed in one register: digit (bits 20..28), leader lane
+    // (15..19), peers below it (10..14) and, on the leader, the counter's
+    // old value (0..9; a warp ranks at most 512 items).
+    static_assert(32 * ITEMS <= 1024, "a warp's counter value must fit 10 bits");
+    constexpr int NB = FULL ? kRadixBits : kRadixBits + 1;
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t li = wl + k * 32;
-    const uint32_t d = (FULL || li < valid) ? digit_of<K, ENC>(sm.keys[li], shift) : (uint32_t)kBins;
-    rd[k] = d << 16;
-    uint32_t* m = sm.mask[k % NT][warp];
-    atomicOr(&m[d], me);
-    __syncwarp();
-    peers[k] = m[d];
-    if constexpr (NT == 1) {
-      __syncwarp();
-      m[d] = 0;
-      __syncwarp();
-    } else {
-      static_assert(NT >= 3, "a round's words are cleared two rounds before reuse");
-      if (k > 0) sm.mask[(k - 1) % NT][warp][rd[k - 1] >> 16] = 0;
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t li = wl + k * 32;
+      const uint32_t d =
+          (FULL || li < valid) ? digit_of<K, ENC>(sm.keys[li], shift) : (uint32_t)kBins;
+      uint32_t eq = kFull;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(kFull, bit);
+        eq &= bit ? bal : ~bal;
+      }
+      const uint32_t below = (uint32_t)__popc(eq & below_me);
+      uint32_t base = 0;
+      if (below == 0) base = atomicAdd(&sm.warp_cnt[warp][d], (uint32_t)__popc(eq));
+      rd[k] = (d << 20) | ((uint32_t)(__ffs(eq) - 1) << 15) | (below << 10) | base;
     }
-  }
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    uint32_t base = 0;
-    if ((peers[k] & below_me) == 0)
-      base = atomicAdd(&sm.warp_cnt[warp][rd[k] >> 16], (uint32_t)__popc(peers[k]));
-    rd[k] |= base;
-  }
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t base = __shfl_sync(kFull, rd[k] & 0x3FFu, (rd[k] >> 15) & 31u);
+      rd[k] = ((rd[k] >> 20) << 16) | (base + ((rd[k] >> 10) & 31u));
+    }
+  } else {
+    uint32_t peers[ITEMS];
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    const uint32_t base = __shfl_sync(kFull, rd[k] & 0xFFFFu, __ffs(peers[k]) - 1);
-    rd[k] = (rd[k] & 0xFFFF0000u) | (base + __popc(peers[k] & below_me));
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t li = wl + k * 32;
+      const uint32_t d =
+          (FULL || li < valid) ? digit_of<K, ENC>(sm.keys[li], shift) : (uint32_t)kBins;
+      rd[k] = d << 16;
+      uint32_t* m = sm.mask[k % NT][warp];
+      atomicOr(&m[d], me);
+      __syncwarp();
+      peers[k] = m[d];
+      if constexpr (NT == 1) {
+        __syncwarp();
+        m[d] = 0;
+        __syncwarp();
+      } else {
+        static_assert(NT >= 3, "a round's words are cleared two rounds before reuse");
+        if (k > 0) sm.mask[(k - 1) % NT][warp][rd[k - 1] >> 16] = 0;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      uint32_t base = 0;
+      if ((peers[k] & below_me) == 0)
+        base = atomicAdd(&sm.warp_cnt[warp][rd[k] >> 16], (uint32_t)__popc(peers[k]));
+      rd[k] |= base;
+    }
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      const uint32_t base = __shfl_sync(kFull, rd[k] & 0xFFFFu, __ffs(peers[k]) - 1);
+      rd[k] = (rd[k] & 0xFFFF0000u) | (base + __popc(peers[k] & below_me));
+    }
   }
   K key[ITEMS];
 #pragma unroll
@@ -596,8 +670,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
       sm.warp_cnt[w][tid] = tile_count;
       tile_count += c;
     }
-    const uint32_t flag = tile == 0 ? kFlagIncl : kFlagAgg;
-    st_relaxed_u32(status + (uint64_t)tile * kBins + tid, (flag << 30) | tile_count);
+    DigitStatus<SW>::publish(status, tile, tid, tile_count);
     uint32_t incl = tile_count;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -657,37 +730,9 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
     }
   }
 
-  // Decoupled look-back, one digit per thread, eight predecessors per step.
+  // Decoupled look-back, one digit per thread.
   if (tid < kBins) {
-    uint32_t excl = 0;
-    if (tile > 0) {
-      constexpr int kBatch = 8;
-      SpinGuard guard(err.abort);
-      int64_t t = (int64_t)tile - 1;
-      bool failed = false, done = false;
-      while (!done) {
-        uint32_t w[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j)
-          w[j] = t - j >= 0 ? ld_relaxed_u32(status + (uint64_t)(t - j) * kBins + tid)
-                            : (kFlagIncl << 30);
-        int used = 0;
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
-          if (done || used < j) break;
-          const uint32_t f = w[j] >> 30;
-          if (f == kFlagNone) break;
-          excl += w[j] & kCountMask;
-          ++used;
-          if (f == kFlagIncl) done = true;
-        }
-        t -= used;
-        if (!done && used < kBatch && guard.expired()) { failed = true; break; }
-      }
-      if (failed) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-      st_relaxed_u32(status + (uint64_t)tile * kBins + tid,
-                     (kFlagIncl << 30) | ((excl + tile_count) & kCountMask));
-    }
+    const uint32_t excl = (uint32_t)DigitStatus<SW>::lookback(status, tile, tid, tile_count, err);
     sm.delta[tid] = digit_offsets[pass * kBins + tid] + excl - sm.tile_start[tid];
   }
   if constexpr (!KEYS_ONLY && !P64) {
@@ -724,11 +769,15 @@ __device__ __forceinline__ void onesweep_tile(OnesweepTmaSmem<K, V, THREADS, ITE
   }
 }
 
-template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool P64>
-__global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THREADS >= 384 ? 2 : 4) : 3)
+// MINB: CTAs per SM the registers are budgeted for (0 = by tile shape);
+// SW: the look-back status word (DigitStatus).
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT, bool P64, int MINB, class SW>
+__global__ void __launch_bounds__(THREADS, MINB > 0 ? MINB
+                                          : NT <= 1 ? (THREADS >= 1024 ? 1 : THREADS >= 384 ? 2 : 4)
+                                                    : 3)
     radix_onesweep_tma_kernel(const PassPlan* __restrict__ plan, int pass, uint32_t n,
                               const uint32_t* __restrict__ digit_offsets,
-                              uint32_t* __restrict__ status, uint32_t* __restrict__ counter,
+                              SW* __restrict__ status, uint32_t* __restrict__ counter,
                               DevErr err) {
   using S = OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>;
   constexpr bool KEYS_ONLY = S::KEYS_ONLY;
@@ -745,7 +794,8 @@ __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THRE
     K* ok = (K*)plan->out_k[0];
     const V* iv = (const V*)plan->in_v[0];
     V* ov = (V*)plan->out_v[0];
-    for (uint32_t i = blockIdx.x * THREADS + tid; i < n; i += gridDim.x * THREADS) {
+    for (uint64_t i = blockIdx.x * (uint64_t)THREADS + tid; i < n;
+         i += (uint64_t)gridDim.x * THREADS) {
       ok[i] = ik[i];
       if constexpr (!KEYS_ONLY) ov[i] = iv[i];
     }
@@ -768,8 +818,12 @@ __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THRE
       if constexpr (!KEYS_ONLY) bulk_load(sm.vals, in_v + (uint64_t)t * TILE, vb, &sm.bar);
     }
   }
-  for (int i = tid; i < (NT + 1) * WARPS * (kBins + 1); i += THREADS)
-    (&sm.mask[0][0][0])[i] = 0;  // mask tables and warp_cnt (adjacent)
+  if constexpr (NT <= 0) {
+    for (int i = tid; i < WARPS * (kBins + 1); i += THREADS) (&sm.warp_cnt[0][0])[i] = 0;
+  } else {
+    for (int i = tid; i < (NT + 1) * WARPS * (kBins + 1); i += THREADS)
+      (&sm.mask[0][0][0])[i] = 0;  // mask tables and warp_cnt (adjacent)
+  }
   __syncthreads();
   const uint32_t tile = sm.tile_id;
   const uint32_t tile_base = tile * TILE;
@@ -779,16 +833,18 @@ __global__ void __launch_bounds__(THREADS, NT == 1 ? (THREADS >= 1024 ? 1 : THRE
   V* out_v = (V*)plan->out_v[pass];
   if (valid == TILE) {
     if (!mbar_wait(&sm.bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
-    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, P64, true>(sm, tile, valid, pass, n, digit_offsets,
-                                                   status, err, out_k, out_v);
+    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, P64, true, SW>(sm, tile, valid, pass, n,
+                                                               digit_offsets, status, err, out_k,
+                                                               out_v);
   } else {
     for (uint32_t i = tid; i < valid; i += THREADS) {
       sm.keys[i] = in_k[tile_base + i];
       if constexpr (!KEYS_ONLY) sm.vals[i] = in_v[tile_base + i];
     }
     __syncthreads();
-    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, P64, false>(sm, tile, valid, pass, n, digit_offsets,
-                                                    status, err, out_k, out_v);
+    onesweep_tile<K, ENC, V, THREADS, ITEMS, NT, P64, false, SW>(sm, tile, valid, pass, n,
+                                                                digit_offsets, status, err, out_k,
+                                                                out_v);
   }
 }
 
@@ -807,25 +863,30 @@ constexpr RadixCfg kRadixCfgs[] = {
     {512, 16, "onesweep 512 threads x 16 keys, 4-byte pairs staged as one 64-bit word"},
     {512, 12, "onesweep 512 threads x 12 keys (6144-key tiles), 64-bit pair staging"},
     {384, 16, "onesweep 384 threads x 16 keys (6144-key tiles), 64-bit pair staging"},
+    {384, 16, "onesweep 384 threads x 16 keys, 64-bit pair staging, ballot peers, 3 CTAs/SM"},
 };
 constexpr int kRadixDefault = 0;    // 64-bit keys or values
 constexpr int kRadixDefault32 = 6;  // 32-bit keys, values of at most 32 bits
 
-template <class K, int ENC, class V, int THREADS, int ITEMS, int NT = 1, bool P64 = false>
+// SW: the look-back status word, 32-bit below 2^30 items, else 64-bit.
+template <class K, int ENC, class V, int THREADS, int ITEMS, int NT = 1, bool P64 = false,
+          int MINB = 0, class SW = uint32_t>
 int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v,
                       uint64_t n, const uint32_t* n_dev) {
   constexpr int PASSES = (int)sizeof(K);
   constexpr int TILE = THREADS * ITEMS;
   constexpr bool KEYS_ONLY = std::is_same<V, uint8_t>::value;
   const uint64_t tiles = (n + TILE - 1) / TILE;
-  if (n >= (1ull << 30))
-    return set_error(MB_ERR_LENGTH_TOO_LARGE, "radix sort supports fewer than 2^30 items", n);
+  if (n > 0xFFFFFFFFull)
+    return set_error(MB_ERR_LENGTH_TOO_LARGE, "radix sort length does not fit in u32", n);
+  if (n >= (uint64_t)DigitStatus<SW>::kMask)
+    return set_error(MB_ERR_LAUNCH, "radix sort: status words too narrow for this length", n);
   // Scratch: [plan][hist P*256][counters + abort word][status P*tiles*256]
   // [tmp keys][tmp values][keys output when none is given]
   const size_t plan_b = ((sizeof(PassPlan) + 255) / 256) * 256;
   const size_t hist_b = (size_t)PASSES * kBins * 4;
   const size_t cnt_b = 256;
-  const size_t status_b = (size_t)PASSES * tiles * kBins * 4;
+  const size_t status_b = (size_t)PASSES * tiles * kBins * sizeof(SW);
   const size_t zero_b = plan_b + hist_b + cnt_b + status_b;
   const size_t tk_b = ((n * sizeof(K) + 255) / 256) * 256;
   const size_t tv_b = KEYS_ONLY ? 0 : ((n * sizeof(V) + 255) / 256) * 256;
@@ -835,7 +896,7 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   PassPlan* plan = (PassPlan*)base;
   uint32_t* hist = (uint32_t*)(base + plan_b);
   uint32_t* counters = (uint32_t*)(base + plan_b + hist_b);
-  uint32_t* status = (uint32_t*)(base + plan_b + hist_b + cnt_b);
+  SW* status = (SW*)(base + plan_b + hist_b + cnt_b);
   K* tmp_k = (K*)(base + zero_b);
   V* tmp_v = KEYS_ONLY ? nullptr : (V*)(base + zero_b + tk_b);
   K* final_k = out_k ? out_k : (K*)(base + zero_b + tk_b + tv_b);
@@ -875,7 +936,7 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
   if (aligned) {
     const size_t smem = sizeof(OnesweepTmaSmem<K, V, THREADS, ITEMS, NT>);
     auto kern = radix_onesweep_tma_kernel<K, ENC, V, THREADS, ITEMS, NT,
-                                          P64 && sizeof(K) == 4 && sizeof(V) == 4>;
+                                          P64 && sizeof(K) == 4 && sizeof(V) == 4, MINB, SW>;
     MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int p = 0; p < PASSES; ++p) {
       {
@@ -888,7 +949,7 @@ int onesweep_sort_cfg(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V
     return MB_OK;
   }
   const size_t smem = onesweep_smem<K, V, THREADS, ITEMS>();
-  auto kern = radix_onesweep_kernel<K, ENC, V, THREADS, ITEMS>;
+  auto kern = radix_onesweep_kernel<K, ENC, V, THREADS, ITEMS, SW>;
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int p = 0; p < PASSES; ++p) {
     {
@@ -905,6 +966,15 @@ template <class K, int ENC, class V>
 int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* out_v, uint64_t n,
                   const uint32_t* n_dev) {
   if (n == 0) return MB_OK;
+  if (n >= (1ull << 30)) {
+    // 2^30 items or more: 64-bit look-back status words, default shapes.
+    if constexpr (sizeof(K) == 4 && sizeof(V) <= 4)
+      return onesweep_sort_cfg<K, ENC, V, 512, 16, 1, true, 0, uint64_t>(ex, in_k, in_v, out_k,
+                                                                         out_v, n, n_dev);
+    else
+      return onesweep_sort_cfg<K, ENC, V, 256, 16, 1, false, 0, uint64_t>(ex, in_k, in_v, out_k,
+                                                                          out_v, n, n_dev);
+  }
   int cfg = ex->tune[MB_TUNE_RADIX];
   if (cfg < 0) cfg = (sizeof(K) == 4 && sizeof(V) <= 4) ? kRadixDefault32 : kRadixDefault;
   switch (cfg) {
@@ -919,6 +989,9 @@ int onesweep_sort(mb_executor* ex, const K* in_k, const V* in_v, K* out_k, V* ou
       return onesweep_sort_cfg<K, ENC, V, 512, 12, 1, true>(ex, in_k, in_v, out_k, out_v, n, n_dev);
     case 8:
       return onesweep_sort_cfg<K, ENC, V, 384, 16, 1, true>(ex, in_k, in_v, out_k, out_v, n, n_dev);
+    case 9:
+      return onesweep_sort_cfg<K, ENC, V, 384, 16, 0, true, 3>(ex, in_k, in_v, out_k, out_v, n,
+                                                               n_dev);
     default: return onesweep_sort_cfg<K, ENC, V, 256, 16, 1>(ex, in_k, in_v, out_k, out_v, n, n_dev);
   }
 }
@@ -938,7 +1011,48 @@ int sort_keys_vals(mb_executor* ex, const void* ik, const void* iv, void* ok, vo
   }
 }
 
+// ---------------------------------------------------- bounded-wait check --
+//
+// Runs the library's own bounded waits against a condition that never comes,
+// so a test can see them end: kind 0, the onesweep digit look-back of tiles
+// 1..blocks, whose tile 0 never publishes (the look-back of tile 1 gives up
+// after the spin limit and sets the launch's abort word; the later tiles
+// then stop waiting as well); kind 1, an mbarrier wait for bulk-copy bytes
+// that no copy delivers.  Each records MB_DEV_ERR_LOOKBACK and returns; no
+// copy is ever in flight.
+__global__ void __launch_bounds__(kBins) bounded_wait_check_kernel(int kind, uint32_t* status,
+                                                                   DevErr err) {
+  if (kind == 0) {
+    const uint64_t tile = blockIdx.x + 1;
+    DigitStatus<uint32_t>::publish(status, tile, threadIdx.x, 1u);
+    DigitStatus<uint32_t>::lookback(status, tile, threadIdx.x, 1u, err);
+  } else {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      mbar_init_fence();
+      mbar_arrive_expect_tx(&bar, 16);  // 16 bytes that never arrive
+      if (!mbar_wait(&bar, 0)) raise_device_error(err, MB_DEV_ERR_LOOKBACK);
+    }
+  }
+}
+
 }  // namespace
+
+int bounded_wait_check(mb_executor* ex, int kind) {
+  MB_TRY(check_exec(ex));
+  if (kind != 0 && kind != 1) return set_error(MB_ERR_LAUNCH, "unknown bounded-wait check");
+  constexpr int kBlocks = 4;
+  Scratch scratch;
+  const size_t status_b = (size_t)(kBlocks + 1) * kBins * 4;
+  MB_TRY(scratch.alloc(ex, 256 + status_b));
+  MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + status_b, ex->stream));
+  const DevErr err{ex->status_dev, scratch.as<uint32_t>()};
+  bounded_wait_check_kernel<<<kind == 0 ? kBlocks : 1, kBins, 0, ex->stream>>>(
+      kind, (uint32_t*)(scratch.as<char>() + 256), err);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
 
 // Radix sort of plain device columns: keys of type `kdt` (32- or 64-bit
 // elements), values of `vsize` bytes (0 = none).  out_k may be null.  With
@@ -963,3 +1077,7 @@ const char* radix_tune_text(int c) {
 }
 
 }  // namespace mb
+
+extern "C" int mb_check_bounded_waits(mb_executor* ex, int kind) {
+  return mb::bounded_wait_check(ex, kind);
+}

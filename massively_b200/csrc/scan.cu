@@ -612,8 +612,10 @@ int scan_entry(mb_executor* ex, const mb_src* in, int op, bool exclusive, const 
 // For callers that cannot allocate device memory during a call.  The
 // look-back scratch (tile ticket, abort word, tile states) lives in this
 // fixed array instead of the executor's pool.  The largest call it admits
-// needs 256 + 32768 tiles * 20 bytes + 64 = 655,680 bytes (2^26 8-byte
-// elements on the register-tiled path); the array is 1 MiB.
+// is 2^26 8-byte elements on the register-tiled path: 32,768 tiles, whose
+// states take 655,616 bytes, plus two group-state arrays of 12,544 bytes
+// and the 256-byte header, 680,960 bytes in all; the array is 1 MiB.  The
+// code checks the exact size of every call against the array.
 constexpr size_t kNoAllocBytes = 1u << 20;
 constexpr uint64_t kNoAllocMax4 = 1ull << 27;  // 4-byte elements
 constexpr uint64_t kNoAllocMax8 = 1ull << 26;  // 8-byte elements
@@ -681,10 +683,11 @@ int scan_noalloc_run(mb_executor* ex, const mb_src& in, int op, const mb_col& ou
   do {                                                                                          \
     if (smem_path) {                                                                            \
       if (smem > 48 * 1024)                                                                     \
-        MB_CUDA(cudaFuncSetAttribute(scan_smem_kernel<T, OPID, PACKED, SmemCfg<T>>,                         \
+        MB_CUDA(cudaFuncSetAttribute(scan_smem_lb_kernel<T, OPID, PACKED, SmemCfg<T>>,          \
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
-      scan_smem_kernel<T, OPID, PACKED, SmemCfg<T>><<<grid, block, smem, ex->stream>>>(                     \
-          (const T*)in.data, (T*)out.data, cap, p, st);                                         \
+      scan_smem_lb_kernel<T, OPID, PACKED, SmemCfg<T>>                                          \
+          <<<grid, kThreads + 32, smem, ex->stream>>>((const T*)in.data, (T*)out.data, cap, p,  \
+                                                      st);                                      \
     } else if (plain) {                                                                         \
       scan_kernel<T, OPID, true, PACKED><<<grid, block, 0, ex->stream>>>(s, out.data, cap, p, st); \
     } else {                                                                                    \

@@ -42,7 +42,11 @@ constexpr int kLoads = 4;
 // warp 0 looks back.
 constexpr int kSegMinBlocks = 4;
 
-enum SegMode : int { kScanIncl = 0, kScanExcl = 1, kReduce = 2 };
+// kReduceTiles: ForEachSegment(Reduce) over offsets without the cross-tile
+// look-back -- each tile reduces the segments that start and end in it and
+// leaves two partial folds for the segments that cross its edges, which
+// seg_reduce_cross_kernel then folds in tile order.
+enum SegMode : int { kScanIncl = 0, kScanExcl = 1, kReduce = 2, kReduceTiles = 3 };
 enum HeadsSrc : int { kHeadsOffsets = 0, kHeadsKeys = 1 };
 
 template <class V>
@@ -107,6 +111,13 @@ struct SegParams {
   uint32_t* count_dev;
   uint32_t* counter;
   DevErr err;
+  // kReduceTiles: per tile, the fold before its first segment start
+  // (part_head), the fold from its last segment start to its end
+  // (part_tail), and the segment that starts at that last start when it goes
+  // on past the tile (tail_seg, ~0u otherwise).
+  V* part_head;
+  V* part_tail;
+  uint32_t* tail_seg;
 };
 
 __device__ __forceinline__ bool key_eq(int dtype, uint64_t a, uint64_t b) {
@@ -297,7 +308,8 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   for (int j = 1; j < kLoads; ++j) rp[j] = op(rp[j - 1], rowtot[j]);
   if (lane == 0) s_warp_total[warp] = rp[kLoads - 1];
   __syncthreads();
-  if (warp == 0) {
+  const bool local = p.mode == kReduceTiles;  // no look-back: every tile starts fresh
+  if (warp == 0 && !local) {
     T agg = s_warp_total[0];
 #pragma unroll
     for (int w = 1; w < kWarps; ++w) agg = op(agg, s_warp_total[w]);
@@ -316,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
     }
   }
   __syncthreads();
-  bool has_pre = tile > 0;
+  bool has_pre = tile > 0 && !local;
   T pre = has_pre ? s_excl : T{0, V(0)};
   for (int w = 0; w < warp; ++w) {
     T t = s_warp_total[w];
@@ -396,11 +408,30 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
         if ((start >= tb && start < te) || (last_tile && start >= te))
           st_cast<V>(p.out_dtype, p.out, s, p.init);
       } else if (end - 1 >= tb && end - 1 < te) {
-        st_cast<V>(p.out_dtype, p.out, s, vop(p.init, stage[end - 1 - tb].v));
+        // (kReduceTiles: a segment that started in an earlier tile is
+        // finished by seg_reduce_cross_kernel)
+        if (!local || start >= tb)
+          st_cast<V>(p.out_dtype, p.out, s, vop(p.init, stage[end - 1 - tb].v));
+      } else if (local && start >= tb && start < te) {
+        p.tail_seg[tile] = (uint32_t)s;  // goes on past this tile
       }
     };
     if (tid == 0 && s_seg[0] != ~0ull) write_seg(s_seg[0]);
     for (uint64_t s = s_seg[1] + tid; s < s_seg[2]; s += kThreads) write_seg(s);
+    if (local) {
+      // The fold before the first segment start (the whole tile when none
+      // starts in it) and the fold from the last start to the tile's end.
+      __shared__ uint32_t s_first;
+      if (tid == 0) s_first = (uint32_t)(te - tb);
+      __syncthreads();
+      if (tid < C::TILE / 32 && s_bits[tid])
+        atomicMin(&s_first, (uint32_t)tid * 32 + __ffs(s_bits[tid]) - 1);
+      __syncthreads();
+      if (tid == 0) {
+        p.part_head[tile] = s_first > 0 ? stage[s_first - 1].v : p.init;
+        p.part_tail[tile] = stage[te - tb - 1].v;
+      }
+    }
   } else {
     // Runs of equal keys: key at the head, value at the tail, index =
     // inclusive head count - 1.
@@ -422,7 +453,30 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
 
 template <class V>
 size_t seg_smem(int mode) {
-  return mode == kReduce ? sizeof(SegVal<V>) * SegCfg<V>::TILE : 0;
+  return mode == kReduce || mode == kReduceTiles ? sizeof(SegVal<V>) * SegCfg<V>::TILE : 0;
+}
+
+// kReduceTiles: the segments that cross tile edges, one thread per tile
+// whose last segment goes on past it: init op (the fold from its start to
+// its tile's end) op (the whole folds of the tiles it covers) op (the fold
+// before the first start of the tile it ends in), left to right, so the
+// result is the same from run to run.
+template <class V>
+__global__ void __launch_bounds__(kThreads)
+    seg_reduce_cross_kernel(const uint32_t* __restrict__ offsets, uint64_t tiles,
+                            uint64_t tile_items, int op, V init, const V* __restrict__ part_head,
+                            const V* __restrict__ part_tail, const uint32_t* __restrict__ tail_seg,
+                            void* out, int out_dtype) {
+  for (uint64_t t = blockIdx.x * (uint64_t)kThreads + threadIdx.x; t < tiles;
+       t += (uint64_t)gridDim.x * kThreads) {
+    const uint32_t s = tail_seg[t];
+    if (s == ~0u) continue;
+    const uint64_t last = ((uint64_t)offsets[s + 1] - 1) / tile_items;  // tile of its last item
+    V acc = part_tail[t];
+    for (uint64_t u = t + 1; u <= last && u < tiles; ++u)
+      acc = op_apply_rt<V>(op, acc, u < last ? part_tail[u] : part_head[u]);
+    st_cast<V>(out_dtype, out, s, op_apply_rt<V>(op, init, acc));
+  }
 }
 
 template <class V>
@@ -438,11 +492,21 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   const size_t state_b =
       pk ? TileState<T, true>::bytes(tiles) : TileState<T, false>::bytes(tiles);
   const size_t lb_b = p.offsets ? ((tiles + 1) * 4 + 255) / 256 * 256 : 0;
+  const bool tiles_mode = p.mode == kReduceTiles;
+  const size_t part_b = tiles_mode ? (tiles * sizeof(V) + 255) / 256 * 256 : 0;
+  const size_t tseg_b = tiles_mode ? (tiles * 4 + 255) / 256 * 256 : 0;
   Scratch scratch;
-  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b));
+  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b + 2 * part_b + tseg_b));
   MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + state_b, ex->stream));
   p.counter = scratch.as<uint32_t>();
   p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
+  if (tiles_mode) {
+    char* q = scratch.as<char>() + 256 + state_b + lb_b;
+    p.part_head = (V*)q;
+    p.part_tail = (V*)(q + part_b);
+    p.tail_seg = (uint32_t*)(q + 2 * part_b);
+    MB_CUDA(cudaMemsetAsync(p.tail_seg, 0xFF, tiles * 4, ex->stream));
+  }
   if (p.offsets) {
     uint32_t* lb = (uint32_t*)(scratch.as<char>() + 256 + state_b);
     MB_CUDA(cudaMemsetAsync(lb, 0xFF, (tiles + 1) * 4, ex->stream));
@@ -453,7 +517,7 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
     p.tile_lb = lb;
   }
   const bool plain = src_plain(in, DTypeOf<V>::value) && (uintptr_t)in.data % 16 == 0 &&
-                     (p.mode == kReduce || (uintptr_t)p.out % 16 == 0);
+                     (p.mode >= kReduce || (uintptr_t)p.out % 16 == 0);
   const Src s = to_src(in);
   const size_t smem = seg_smem<V>(p.mode);
   char* state_base = scratch.as<char>() + 256;
@@ -485,6 +549,13 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   }
 #undef MB_SEG_LAUNCH
   MB_CUDA(cudaGetLastError());
+  if (tiles_mode) {
+    const unsigned g = (unsigned)std::min<uint64_t>((tiles + kThreads - 1) / kThreads, 4096);
+    seg_reduce_cross_kernel<V><<<std::max(1u, g), kThreads, 0, ex->stream>>>(
+        p.offsets, tiles, C::TILE, p.op, p.init, p.part_head, p.part_tail, p.tail_seg, p.out,
+        p.out_dtype);
+    MB_CUDA(cudaGetLastError());
+  }
   return MB_OK;
 }
 
@@ -862,7 +933,10 @@ int mb_seg_reduce(mb_executor* ex, const mb_src* values, const uint32_t* offsets
   if (!op_commutative(op) && op != MB_OP_TAKE_RIGHT && op != MB_OP_TAKE_LEFT)
     return set_error(MB_ERR_LAUNCH, "operator not supported");
   if (values->len == 0) return segment_count ? mb_fill(ex, init, out) : MB_OK;
-  return seg_entry(ex, values, op, kReduce, init, out.data, out.dtype, offsets, segment_count,
+  // Tuning (MB_TUNE_SEG): 0 = tile-local folds plus the crossing-segment
+  // pass (default), 1 = the segmented scan's look-back carried across tiles.
+  const int mode = ex->tune[MB_TUNE_SEG] == 1 ? kReduce : kReduceTiles;
+  return seg_entry(ex, values, op, mode, init, out.data, out.dtype, offsets, segment_count,
                    nullptr, nullptr, 0, nullptr);
 }
 

@@ -17,6 +17,7 @@ int mb_tune_config_count(int family) {
   switch (family) {
     case MB_TUNE_RADIX: return radix_tune_count();
     case MB_TUNE_SCAN: return 3;
+    case MB_TUNE_SEG: return 2;
     case MB_TUNE_REDUCE: case MB_TUNE_SELECT: return 1;
     default: return 0;
   }
@@ -28,6 +29,10 @@ const char* mb_tune_describe(int family, int config) {
     return "scan one 32 KB tile per CTA, warp 0 runs the look-back after the tile scan";
   if (family == MB_TUNE_SCAN && config == 2)
     return "scan one 64 KB tile per CTA, a ninth warp runs the look-back";
+  if (family == MB_TUNE_SEG && config == 0)
+    return "segmented reduce: tile-local folds, then one pass over the segments crossing tiles";
+  if (family == MB_TUNE_SEG && config == 1)
+    return "segmented reduce: the segmented scan with its look-back carried across tiles";
   if (config == 0) {
     switch (family) {
       case MB_TUNE_SCAN: return "scan one 32 KB tile per CTA, a ninth warp runs the look-back";

@@ -45,23 +45,45 @@ def group_by(exec: Executor, keys: DeviceVec, values: DeviceVec, flag: DeviceVec
 class Captured:
     """`fn(exec)` captured once into a CUDA graph; `replay()` relaunches it on
     the current stream.  The outputs `fn` returned are kept (their buffers
-    are rewritten by each replay)."""
+    are rewritten by each replay).
+
+    Every buffer the calls allocate (outputs, intermediates, device counts)
+    is a slice of one arena (runtime.Arena) that this object owns: a warm-up
+    run records the sizes, the arena is allocated before capture, and the
+    captured calls take their storage from it.  So no allocation of torch's
+    happens inside the capture, the outputs live exactly as long as the
+    graph that writes them, and `release()` (or dropping this object) frees
+    graph and buffers together.  The library's own per-call scratch is
+    stream-ordered pool memory, which the capture turns into graph
+    allocations."""
 
     def __init__(self, exec: Executor, fn, warmup: int = 1):
+        from .runtime import Arena
         self.exec = exec
+        self.arena = Arena()
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
             exec.bind_current_stream()
-            for _ in range(warmup):  # loads kernels and fills the pools outside capture
+            with self.arena.on(exec):  # records the sizes of every allocation
+                fn(exec)
+            for _ in range(warmup - 1):  # loads kernels and fills the pools outside capture
                 fn(exec)
         torch.cuda.current_stream().wait_stream(side)
         exec.sync()
+        self.arena.allocate(exec.device)
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
             exec.bind_current_stream()
-            self.outputs = fn(exec)
+            with self.arena.on(exec):
+                self.outputs = fn(exec)
         exec.bind_current_stream()
 
     def replay(self) -> None:
         self.graph.replay()
+
+    def release(self) -> None:
+        """Frees the graph, then the arena its outputs live in."""
+        self.graph = None
+        self.outputs = None
+        self.arena = None

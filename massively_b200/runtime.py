@@ -191,8 +191,15 @@ class Executor:
         """Executor::alloc: uninitialised device storage of `n` items."""
         if n > MINDEX_MAX:
             raise LengthTooLarge(n)
-        t = torch.empty(int(n), dtype=NP_TO_TORCH[np.dtype(dtype)], device=f"cuda:{self.device}")
-        return DeviceVec(self, t)
+        return DeviceVec(self, self.storage(NP_TO_TORCH[np.dtype(dtype)], int(n)))
+
+    def storage(self, tdtype: torch.dtype, n: int) -> torch.Tensor:
+        """`n` items of device storage: a fresh tensor, or the next slice of
+        the executor's arena while one is set (Arena)."""
+        a = getattr(self, "_arena", None)
+        if a is None:
+            return torch.empty(n, dtype=tdtype, device=f"cuda:{self.device}")
+        return a.take(tdtype, n, self.device)
 
     def zeros(self, dtype, n: int) -> "DeviceVec":
         v = self.alloc(dtype, n)
@@ -260,6 +267,62 @@ class Executor:
         used, res = C.c_uint64(), C.c_uint64()
         check(self._lib.mb_pool_stats(self._h, C.byref(used), C.byref(res)))
         return int(used.value), int(res.value)
+
+
+class Arena:
+    """Storage for the calls made while it is set on an executor
+    (`with arena.on(exec):`): in "record" mode allocations are ordinary
+    tensors and only their sizes are noted; in "serve" mode they are
+    consecutive 256-byte-aligned slices of one buffer allocated beforehand.
+    A CUDA graph captured in "serve" mode (pipeline.Captured) therefore makes
+    no allocation of torch's during capture: every buffer it reads or writes
+    belongs to the arena, which lives exactly as long as its owner keeps it."""
+
+    ALIGN = 256
+
+    def __init__(self):
+        self.sizes: list[int] = []
+        self.buf: torch.Tensor | None = None
+        self.off = 0
+
+    @staticmethod
+    def _round(nbytes: int) -> int:
+        return (nbytes + Arena.ALIGN - 1) // Arena.ALIGN * Arena.ALIGN
+
+    def allocate(self, device: int) -> None:
+        """Switches from recording to serving: one buffer for the sizes
+        recorded so far."""
+        total = sum(self._round(s) for s in self.sizes)
+        self.buf = torch.empty(max(total, self.ALIGN), dtype=torch.uint8, device=f"cuda:{device}")
+        self.off = 0
+
+    def take(self, tdtype: torch.dtype, n: int, device: int) -> torch.Tensor:
+        nbytes = n * torch.empty(0, dtype=tdtype).element_size()
+        if self.buf is None:
+            self.sizes.append(nbytes)
+            return torch.empty(n, dtype=tdtype, device=f"cuda:{device}")
+        end = self.off + self._round(nbytes)
+        if end > self.buf.numel():
+            raise RuntimeError("arena exhausted: the calls allocate more than when recorded")
+        t = self.buf[self.off:self.off + nbytes].view(tdtype)
+        self.off = end
+        return t
+
+    class _On:
+        def __init__(self, arena, exec):
+            self.arena, self.exec = arena, exec
+
+        def __enter__(self):
+            self.prev = getattr(self.exec, "_arena", None)
+            self.exec._arena = self.arena
+            return self.arena
+
+        def __exit__(self, *exc):
+            self.exec._arena = self.prev
+            return False
+
+    def on(self, exec: "Executor"):
+        return Arena._On(self, exec)
 
 
 class DeviceVec:

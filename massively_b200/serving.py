@@ -48,8 +48,8 @@ class Request:
     def bytes_needed(self) -> int:
         # inputs + outputs + the kernels' scratch on the device (the sort's
         # ping-pong buffers and look-back states, the run-count scratch of
-        # reduce_by_key)
-        return {SORT: 26, SCAN: 9, RBK: 28}[self.kind] * self.n
+        # reduce_by_key and, when coalesced, each run's first row)
+        return {SORT: 26, SCAN: 9, RBK: 32}[self.kind] * self.n
 
 
 def make_trace(rate: float = 20_000.0, duration: float = 1.0, lo_log2: int = 10,
@@ -87,12 +87,14 @@ def materialize_inputs(exec: Executor, r: Request, into: dict | None = None) -> 
     elif r.kind == SCAN:
         check(N.lib().mb_random_uniform_u32(exec.handle, 0, 1000, r.seed, 0, cols["x"].to_col()))
     else:
-        # sorted keys in runs of 8 (the group-by shape after sort_by_key);
-        # values are integers below 2^20 held as f32
-        copy(exec, lazy.RepeatEach(lazy.counting(r.seed & 0xFFFF).take((r.n + 7) // 8), r.n,
-                                   a=8), cols["keys"])
+        # keys 0 / 1 from the PCG stream: runs of adjacent equal keys with
+        # irregular (geometric) lengths; values are integers below 2^16 held
+        # as f32, so any run shorter than 256 sums exactly in f32
+        check(N.lib().mb_random_uniform_u32(exec.handle, 0, 1, r.seed ^ 0x5bd1e995, 0,
+                                            cols["keys"].to_col()))
         v = exec.alloc(np.uint32, r.n)
-        check(N.lib().mb_random_uniform_u32(exec.handle, 0, 1 << 20, r.seed, 0, v.to_col()))
+        check(N.lib().mb_random_uniform_u32(exec.handle, 0, (1 << 16) - 1, r.seed, 0,
+                                            v.to_col()))
         copy(exec, lazy.cast(v, np.float32), cols["values"])
     r.inputs = cols
 
@@ -131,9 +133,15 @@ def _offsets(exec, reqs):
     return exec.to_device(off), off
 
 
-def run_coalesced(exec: Executor, reqs: list[Request], batch: dict) -> None:
+def run_coalesced(exec: Executor, reqs: list[Request], batch: dict):
     """Several small requests of one kind, whose inputs sit back to back in
-    `batch` (materialize_batch), in one segmented launch."""
+    `batch` (materialize_batch), in one segmented launch.
+
+    Returns None when every request's outputs are set, or a callable that
+    sets them and may only be called once the launch's work has completed
+    (reduce_by_key: where each request's runs start in the batch's output is
+    known only on the device; it is copied to pinned host memory behind the
+    launch and read when the launch retires)."""
     from . import seg, vector
     kind = reqs[0].kind
     dev_off, host_off = _offsets(exec, reqs)
@@ -154,16 +162,34 @@ def run_coalesced(exec: Executor, reqs: list[Request], batch: dict) -> None:
             r.outputs = {"keys": sk.slice(a, b), "values": sv.slice(a, b)}
     else:
         keys, vals = batch["keys"], batch["values"]
-        # runs break at request boundaries as well as at key changes
-        k, v = vector.reduce_by_key_segmented(exec, keys, vals, O.Equal, np.float32(0), O.Add,
-                                              dev_off)
-        # runs come out grouped by request, in order; the synthetic keys hold
-        # runs of 8, so request i owns ceil(n_i / 8) of them
-        counts = [int(math.ceil(r.n / 8)) for r in reqs]
-        starts = np.concatenate([[0], np.cumsum(counts)])
-        for i, r in enumerate(reqs):
-            a, b = int(starts[i]), int(starts[i + 1])
-            r.outputs = {"keys": k.slice(a, b), "values": v.slice(a, b)}
+        # Runs break at request boundaries as well as at key changes, and
+        # come out grouped by request, in order.  A second value column
+        # (MIN over the row index) gives each run's first row; request i's
+        # runs then start at lower_bound(first rows, offset_i).
+        k, v, first = _rbk_with_first_rows(exec, keys, vals, dev_off, int(host_off[-1]))
+        starts = vector.lower_bound(exec, first, dev_off)
+        host = torch.empty(len(reqs) + 1, dtype=torch.int32, pin_memory=True)
+        host.copy_(starts.tensor.view(torch.int32), non_blocking=True)
+
+        def finish():
+            st = host.numpy()
+            for i, r in enumerate(reqs):
+                a, b = int(st[i]), int(st[i + 1])
+                r.outputs = {"keys": k.slice(a, b), "values": v.slice(a, b)}
+        return finish
+    return None
+
+
+def _rbk_with_first_rows(exec, keys, vals, dev_off, total):
+    """reduce_by_key_segmented of `vals` (ADD) that also returns each run's
+    first row index."""
+    from . import vector
+    from .iter import Zip
+    k, z = vector.reduce_by_key_segmented(
+        exec, keys, Zip(vals, lazy.counting(0).take(total)), O.Equal,
+        (np.float32(0), np.uint32(0xFFFFFFFF)), (O.Add, O.Min), dev_off)
+    v, first = z.into_columns()
+    return k, v, first
 
 
 # ---------------------------------------------------------------- loops ----
@@ -224,7 +250,7 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
     small: dict[str, deque[Request]] = {SORT: deque(), SCAN: deque(), RBK: deque()}
     taken: set[int] = set()
     nwait = 0
-    inflight = []               # (event, [requests], bytes, stream index)
+    inflight = []               # (event, [requests], bytes, stream index, finish)
     load = [0] * streams        # launches in flight per stream
     used = max_used = launches = nxt = done_count = 0
 
@@ -235,9 +261,11 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
 
     while done_count < len(reqs):
         still = []
-        for ev, group, b, si in inflight:
+        for ev, group, b, si, finish in inflight:
             if ev.query():
                 t = clock.gpu_time(ev)
+                if finish is not None and keep_outputs:
+                    finish()
                 for r in group:
                     r.done = t
                     if not keep_outputs:
@@ -247,7 +275,7 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
                 done_count += len(group)
                 load[si] -= 1
             else:
-                still.append((ev, group, b, si))
+                still.append((ev, group, b, si, finish))
         inflight = still
         now = clock.now()
         while nxt < len(reqs) and reqs[nxt].arrival <= now:
@@ -285,11 +313,12 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
             nwait -= len(group)
             with torch.cuda.stream(pool[si]):
                 exec.bind_current_stream()
+                finish = None
                 if len(group) == 1:
                     materialize_inputs(exec, group[0])
                     run_single(exec, group[0])
                 else:
-                    run_coalesced(exec, group, materialize_batch(exec, group))
+                    finish = run_coalesced(exec, group, materialize_batch(exec, group))
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record()
             used += b
@@ -297,7 +326,7 @@ def serve(exec: Executor, reqs: list[Request], budget_bytes: int = 40 << 30,
             load[si] += 1
             launches += 1
             launched = True
-            inflight.append((ev, group, b, si))
+            inflight.append((ev, group, b, si, finish))
         if not launched:
             if not inflight and not nwait and nxt < len(reqs):
                 time.sleep(max(0.0, min(1e-3, reqs[nxt].arrival - clock.now())))

@@ -91,7 +91,9 @@ def _first_len_dev(*xs):
 
 
 def _count_buffer(exec: Executor) -> torch.Tensor:
-    return torch.zeros(1, dtype=torch.uint32, device=f"cuda:{exec.device}")
+    t = exec.storage(torch.uint32, 1)
+    t.zero_()
+    return t
 
 
 def _p32(t: torch.Tensor):
@@ -137,6 +139,37 @@ def fill(exec: Executor, value, output: DeviceVec) -> None:
     """vector::fill (selection.rs:321)."""
     buf = scalar_buffer(value, output.dtype)
     check(_L().mb_fill(exec.handle, buf, output.to_col()))
+
+
+def replace_where(exec: Executor, value, stencil, output) -> None:
+    """vector::replace_where (massively/src/api/algorithm/selection.rs:363):
+    output items whose stencil flag is non-zero become `value` (a tuple for
+    zipped outputs); the others keep theirs."""
+    _check_owner(exec, stencil, output)
+    from .runtime import value_bits
+    cols = _columns(output)
+    vals = list(value) if isinstance(value, (tuple, list)) else [value]
+    if len(vals) != len(cols):
+        raise LengthMismatch(len(cols), len(vals))
+    keep = []
+    st = lower(exec, stencil, keep)
+    bits = (C.c_uint64 * len(cols))(*[value_bits(v, c.dtype) for v, c in zip(vals, cols)])
+    check(_L().mb_replace_where(exec.handle, bits, C.byref(st), _cols(cols), len(cols)))
+
+
+def transform_where(exec: Executor, input, unary, stencil, output) -> None:
+    """vector::transform_where (selection.rs:436): output[i] = unary(input[i])
+    where the stencil flag is non-zero; other items keep theirs.  `unary` a
+    built-in op (op.UnaryOp) applied to every column of a zipped input."""
+    _check_owner(exec, input, stencil, output)
+    ins, outs = _columns(input), _columns(output)
+    if len(ins) != len(outs):
+        raise LengthMismatch(len(ins), len(outs))
+    keep = []
+    views = [Map(c, unary, o.dtype) for c, o in zip(ins, outs)]
+    srcs = (N.mb_src * len(views))(*[lower(exec, v, keep) for v in views])
+    st = lower(exec, stencil, keep)
+    check(_L().mb_transform_where(exec.handle, srcs, len(views), C.byref(st), _cols(outs)))
 
 
 # ----------------------------------------------------------------- scan --
@@ -624,12 +657,14 @@ def _opt(r):
 def count(exec: Executor, input) -> int:
     """vector::count (massively/src/api/algorithm/predicate.rs:53): the
     logical number of items -- a device length when the input carries one
-    (read back), else its length."""
+    (read back), else its length.  For zipped columns it is the smallest
+    logical length of the columns (the rows all of them hold)."""
     _check_owner(exec, input)
-    c = _columns(input)[0]
-    if isinstance(c, DeviceVec):
-        return c.logical_len()
-    return _len(input)
+    n = _len(input)
+    for c in _columns(input):
+        if isinstance(c, DeviceVec):
+            n = min(n, c.logical_len())
+    return n
 
 
 def count_if(exec: Executor, input, pred) -> int:

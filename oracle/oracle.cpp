@@ -22,6 +22,8 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "../include/massively_b200.h"
@@ -642,6 +644,21 @@ void orc_gather(const void* src, uint64_t width, const uint32_t* idx, const uint
     if (!stencil || stencil[i])
       std::memcpy((uint8_t*)out + i * width, (const uint8_t*)src + (uint64_t)idx[i] * width, width);
 }
+// replace_where (verification/oracle/src/vector.rs:277-283): out[i] = value
+// where stencil[i] != 0.  transform_where (vector.rs:20-31) is the same loop
+// over the operator's results: out[i] = src[i] where stencil[i] != 0, with
+// `src` already holding op(input) (orc_masked_copy).
+void orc_replace_where(const void* value, uint64_t width, const uint32_t* stencil, uint64_t n,
+                       void* out) {
+  for (uint64_t i = 0; i < n; ++i)
+    if (stencil[i] != 0) std::memcpy((uint8_t*)out + i * width, value, width);
+}
+void orc_masked_copy(const void* src, uint64_t width, const uint32_t* stencil, uint64_t n,
+                     void* out) {
+  for (uint64_t i = 0; i < n; ++i)
+    if (stencil[i] != 0)
+      std::memcpy((uint8_t*)out + i * width, (const uint8_t*)src + i * width, width);
+}
 void orc_scatter(const void* src, uint64_t width, const uint32_t* idx, const uint32_t* stencil,
                  uint64_t n, void* out) {
   for (uint64_t i = 0; i < n; ++i)
@@ -682,6 +699,59 @@ int orc_radix_perm(int nkeys, const int* dts, const void* const* cols, uint64_t 
     return false;
   });
   for (uint64_t i = 0; i < n; ++i) perm[i] = (uint32_t)order[i];
+  return 0;
+}
+// The same order for one key column at full benchmark sizes, on `threads`
+// host threads.  A stable sort's result is unique: it is the sort by
+// (encoded key, input index), which has no ties.  So the items are sorted as
+// (encoded key, index) pairs -- in chunks, one per thread, then merged
+// pairwise -- and the permutation equals orc_radix_perm's exactly.
+int orc_radix_perm_par(int dt, const void* col, uint64_t n, int threads, uint32_t* perm) {
+  if (n > 0xFFFFFFFFull) return -1;
+  if (threads < 1) threads = 1;
+  std::vector<std::pair<uint64_t, uint32_t>> v(n), w(n);
+  auto enc = [&](uint64_t i) -> uint64_t {
+    switch (dt) {
+      case MB_U32: return radix_encode<uint32_t>(((const uint32_t*)col)[i]);
+      case MB_U64: return radix_encode<uint64_t>(((const uint64_t*)col)[i]);
+      case MB_I32: return radix_encode<int32_t>(((const int32_t*)col)[i]);
+      case MB_I64: return radix_encode<int64_t>(((const int64_t*)col)[i]);
+      case MB_F32: return radix_encode<float>(((const float*)col)[i]);
+      case MB_F64: return radix_encode<double>(((const double*)col)[i]);
+    }
+    return 0;
+  };
+  if (dt != MB_U32 && dt != MB_U64 && dt != MB_I32 && dt != MB_I64 && dt != MB_F32 && dt != MB_F64)
+    return -1;
+  std::vector<uint64_t> bounds;
+  for (int t = 0; t <= threads; ++t) bounds.push_back(n * (uint64_t)t / (uint64_t)threads);
+  {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+      pool.emplace_back([&, t] {
+        for (uint64_t i = bounds[t]; i < bounds[t + 1]; ++i) v[i] = {enc(i), (uint32_t)i};
+        std::sort(v.begin() + bounds[t], v.begin() + bounds[t + 1]);
+      });
+    for (auto& th : pool) th.join();
+  }
+  // pairwise merges of neighbouring sorted runs until one is left
+  while (bounds.size() > 2) {
+    std::vector<uint64_t> next;
+    std::vector<std::thread> pool;
+    for (size_t r = 0; r + 1 < bounds.size(); r += 2) {
+      const uint64_t a = bounds[r], b = bounds[r + 1];
+      const uint64_t c = r + 2 < bounds.size() ? bounds[r + 2] : b;
+      next.push_back(a);
+      pool.emplace_back([&, a, b, c] {
+        std::merge(v.begin() + a, v.begin() + b, v.begin() + b, v.begin() + c, w.begin() + a);
+      });
+    }
+    next.push_back(n);
+    for (auto& th : pool) th.join();
+    v.swap(w);
+    bounds.swap(next);
+  }
+  for (uint64_t i = 0; i < n; ++i) perm[i] = v[i].second;
   return 0;
 }
 int orc_run_heads(int kdt, const void* keys, uint64_t n, int key_eq, uint8_t* heads) {

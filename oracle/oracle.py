@@ -64,8 +64,11 @@ def _declare(L: C.CDLL) -> None:
         "orc_partition": (i64, [i32, vp, u64, i32, vp]),
         "orc_gather": (None, [vp, u64, vp, vp, u64, vp]),
         "orc_scatter": (None, [vp, u64, vp, vp, u64, vp]),
+        "orc_replace_where": (None, [vp, u64, vp, u64, vp]),
+        "orc_masked_copy": (None, [vp, u64, vp, u64, vp]),
         "orc_sort_perm": (i32, [i32, vp, u64, i32, vp]),
         "orc_radix_perm": (i32, [i32, vp, vp, u64, vp]),
+        "orc_radix_perm_par": (i32, [i32, vp, u64, i32, vp]),
         "orc_run_heads": (i32, [i32, vp, u64, i32, vp]),
         "orc_adjacent_heads": (i32, [i32, vp, u64, i32, vp]),
         "orc_runs_reduce": (i64, [i32, vp, u64, vp, i32, vp, vp]),
@@ -269,6 +272,26 @@ def scatter(src, idx, out, stencil=None):
     return out
 
 
+def replace_where(value, stencil, out):
+    """vector.rs:277-283: a new array, `value` where stencil[i] != 0."""
+    o = _c(np.array(out, copy=True))
+    st = _c(np.asarray(stencil, np.uint32))
+    v = _scalar(value, o.dtype)
+    lib().orc_replace_where(_p(v), o.itemsize, _p(st), o.size, _p(o))
+    return o
+
+
+def transform_where(source, op, stencil, out):
+    """vector.rs:20-31: a new array, op(source[i]) where stencil[i] != 0;
+    `op` is a host function mapping an array to its results (the operator
+    applied item by item)."""
+    o = _c(np.array(out, copy=True))
+    res = _c(np.asarray(op(np.asarray(source)), dtype=o.dtype))
+    st = _c(np.asarray(stencil, np.uint32))
+    lib().orc_masked_copy(_p(res), o.itemsize, _p(st), o.size, _p(o))
+    return o
+
+
 def sort_perm(keys, less: str = "less") -> np.ndarray:
     """Stable comparator order (vector.rs:483-491, 666-680)."""
     keys = _c(keys)
@@ -301,6 +324,20 @@ def radix_perm(key_cols) -> np.ndarray:
     ptrs = (C.c_void_p * len(key_cols))(*[k.ctypes.data for k in key_cols])
     perm = np.empty(n, np.uint32)
     lib().orc_radix_perm(len(key_cols), _p(dts), C.cast(ptrs, C.c_void_p), n, _p(perm))
+    return perm
+
+
+def radix_perm_par(keys, threads: int | None = None) -> np.ndarray:
+    """radix_perm of one key column on several host threads, for full
+    benchmark sizes: the same permutation (a stable order is the order by
+    (encoded key, input index), which the threads sort and merge)."""
+    import os
+    keys = _c(keys)
+    perm = np.empty(keys.size, np.uint32)
+    rc = lib().orc_radix_perm_par(_dt(keys), _p(keys), keys.size,
+                                  int(threads or os.cpu_count() or 1), _p(perm))
+    if rc != 0:
+        raise ValueError("radix_perm_par takes one 32- or 64-bit key column below 2^32 items")
     return perm
 
 

@@ -3,7 +3,8 @@
 Each entry cites the test (path inside the massively project) whose inputs
 and asserted outputs it carries.  The oracle is pinned against every entry
 (tests/test_oracle_golden.py) and the CUDA path is checked against the same
-entries (tests/test_known_answers_gpu.py).  No generator script: the values
+entries (the `test_known_answers*` tests of the tests/test_*_gpu.py files).
+No generator script: the values
 are the literal inputs and expected outputs of those tests.
 """
 import numpy as np
@@ -106,6 +107,28 @@ SCATTER = [
          values=np.array([10, 20, 30], U32), idx=np.array([2, 0, 1], U32),
          stencil=np.array([1, 0, 1], U32), out=np.array([99, 99, 99], U32),
          want=np.array([99, 30, 10], U32)),
+]
+
+REPLACE_WHERE = [
+    # api/algorithm/selection.rs:349-361 (doctest)
+    dict(src="massively/src/api/algorithm/selection.rs:349-361", value=99,
+         stencil=np.array([0, 1, 0, 1], U32), out=np.array([10, 20, 30, 40], U32),
+         want=np.array([10, 99, 30, 99], U32)),
+    # tests/vector/api/owned.rs:301-310 (value 3 = a reduced total)
+    dict(src="massively/tests/vector/api/owned.rs:301-310", value=3,
+         stencil=np.array([0, 1, 0], U32), out=np.array([8, 8, 8], U32),
+         want=np.array([8, 3, 8], U32)),
+]
+
+TRANSFORM_WHERE = [
+    # api/algorithm/selection.rs:397-434 (doctest; AddOne)
+    dict(src="massively/src/api/algorithm/selection.rs:397-434", op=lambda x: x + 1,
+         x=np.array([1, 2, 3], U32), stencil=np.array([1, 0, 1], U32),
+         out=np.array([100, 100, 100], U32), want=np.array([2, 100, 4], U32)),
+    # tests/vector/api/iter.rs:31-46 (Identity under an all-true stencil)
+    dict(src="massively/tests/vector/api/iter.rs:31-46", op=lambda x: x,
+         x=np.array([1, 2, 3], U32), stencil=np.array([1, 1, 1], U32),
+         out=np.array([0, 0, 0], U32), want=np.array([1, 2, 3], U32)),
 ]
 
 SORT = [

@@ -64,6 +64,15 @@ def test_gather_scatter_known_answers(orc):
         np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
 
 
+def test_replace_transform_where_known_answers(orc):
+    for case in K.REPLACE_WHERE:
+        got = orc.replace_where(case["value"], case["stencil"], case["out"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+    for case in K.TRANSFORM_WHERE:
+        got = orc.transform_where(case["x"], case["op"], case["stencil"], case["out"])
+        np.testing.assert_array_equal(got, case["want"], err_msg=case["src"])
+
+
 def test_ordering_known_answers(orc):
     for case in K.SORT:
         np.testing.assert_array_equal(orc.sort(case["x"]), case["want"], err_msg=case["src"])

@@ -306,3 +306,16 @@ def test_count_logical_length(ex):
     sel = vector.copy_where(ex, ex.to_device(x), ex.to_device(st))
     assert vector.count(ex, sel) == int(st.sum())
     assert vector.count(ex, lazy.counting(0).take(77)) == 77
+
+
+def test_count_of_zipped_columns_is_the_shortest_logical_length(ex):
+    """A zip whose later column carries the shorter device length counts the
+    rows every column holds."""
+    from massively_b200 import vector
+    from massively_b200.iter import Zip
+    n = 5000
+    a = ex.to_device(np.arange(n, dtype=np.uint32))
+    b = ex.to_device(np.arange(n, dtype=np.uint32)).with_len_dev(
+        ex.to_device(np.array([1234], np.uint32)).tensor)
+    assert vector.count(ex, Zip(a, b)) == 1234
+    assert vector.count(ex, Zip(b, a)) == 1234

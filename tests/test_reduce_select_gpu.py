@@ -225,3 +225,66 @@ def test_random_streams_match_oracle(ex):
     mb.runtime.check(N.lib().mb_random_uniform_u64(ex.handle, 0, 2**64 - 1, 2, 0,
                                                    out64.to_col()))
     np.testing.assert_array_equal(ex.to_host(out64), orc.uniform_u64(0, 2**64 - 1, 2, n))
+
+
+# ----------------------------------------------- replace / transform where --
+
+def test_replace_where_known_answers_and_seeded(ex):
+    """vector::replace_where: the reference's doctest and owned-value test,
+    then seeded stencils over every element width and a zipped output."""
+    from massively_b200 import lazy, op, vector, zip2
+    for case in K.REPLACE_WHERE:
+        out = ex.to_device(case["out"])
+        vector.replace_where(ex, np.uint32(case["value"]), ex.to_device(case["stencil"]), out)
+        np.testing.assert_array_equal(ex.to_host(out), case["want"], err_msg=case["src"])
+    for dtype in (np.uint8, np.int16, np.uint32, np.float32, np.int64, np.float64):
+        n = 70_001
+        base = seeded(dtype, n, 5)
+        st = (seeded(np.uint32, n, 6) % 3 == 0).astype(np.uint32)
+        value = np.array([7], dtype)[0]
+        out = ex.to_device(base)
+        vector.replace_where(ex, value, ex.to_device(st), out)
+        np.testing.assert_array_equal(ex.to_host(out).view(np.uint8),
+                                      orc.replace_where(value, st, base).view(np.uint8))
+    # zipped output, lazy stencil (is_odd over a column)
+    n = 4099
+    a, b = seeded(np.uint32, n, 7), seeded(np.float32, n, 8)
+    key = seeded(np.uint32, n, 9)
+    oa, ob = ex.to_device(a), ex.to_device(b)
+    vector.replace_where(ex, (np.uint32(5), np.float32(-1.5)),
+                         lazy.map(ex.to_device(key), op.IsOdd), zip2(oa, ob))
+    st = (key & 1).astype(np.uint32)
+    np.testing.assert_array_equal(ex.to_host(oa), orc.replace_where(5, st, a))
+    np.testing.assert_array_equal(ex.to_host(ob), orc.replace_where(np.float32(-1.5), st, b))
+
+
+def test_transform_where_seeded_and_errors(ex):
+    """vector::transform_where with built-in unary operators: op(x) where the
+    stencil is set, the output kept elsewhere; length errors as massively's
+    (core/selection.rs:538-551)."""
+    from massively_b200 import op, vector
+    from massively_b200.runtime import LengthMismatch
+    for dtype, unary, host_op in [(np.int32, op.Negate, lambda x: -x),
+                                  (np.uint32, op.BitNot, lambda x: ~x),
+                                  (np.float64, op.Abs, np.abs),
+                                  (np.uint64, op.IsEven, lambda x: (x & 1) == 0)]:
+        n = 100_003
+        x = seeded(dtype, n, 10)
+        st = (seeded(np.uint32, n, 11) & 1).astype(np.uint32)
+        out_dt = np.uint32 if unary is op.IsEven else dtype
+        base = seeded(out_dt, n, 12)
+        out = ex.to_device(base)
+        vector.transform_where(ex, ex.to_device(x), unary, ex.to_device(st), out)
+        want = orc.transform_where(x, host_op, st, base)
+        np.testing.assert_array_equal(ex.to_host(out).view(np.uint8), want.view(np.uint8))
+    d3 = ex.to_device(np.arange(3, dtype=np.uint32))
+    d4 = ex.to_device(np.arange(4, dtype=np.uint32))
+    with pytest.raises(LengthMismatch) as e:
+        vector.transform_where(ex, d3, op.Identity, d4, ex.to_device(np.zeros(3, np.uint32)))
+    assert (e.value.left, e.value.right) == (3, 4)
+    with pytest.raises(LengthMismatch) as e:
+        vector.transform_where(ex, d3, op.Identity, d3, ex.to_device(np.zeros(4, np.uint32)))
+    assert (e.value.left, e.value.right) == (3, 4)
+    with pytest.raises(LengthMismatch) as e:
+        vector.replace_where(ex, np.uint32(1), d3, ex.to_device(np.zeros(4, np.uint32)))
+    assert (e.value.left, e.value.right) == (3, 4)

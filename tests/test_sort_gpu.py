@@ -236,3 +236,43 @@ def test_autotune_records_and_selects_fastest(tmp_path):
     np.testing.assert_array_equal(ex.to_host(sv), orc.radix_perm([keys]))
     tune.set_config(ex, "radix", -1)
     ex.sync()
+
+
+def test_radix_sort_beyond_2e30_items(ex):
+    """massively's length contract is any length that fits u32
+    (massively/src/lib.rs:82, core/runtime.rs:14-19): 2^30 + 5 (u32 key,
+    u32 value = index) pairs, with 60% of the keys sharing their second byte
+    (one digit bucket then holds more than 2^29 items).  The result is the
+    unique stable order: output keys are the input keys at the output
+    values, (key, value) strictly increases (sorted, and stable since the
+    values are the input positions), and the values are a permutation."""
+    import torch
+
+    import bench
+    from massively_b200 import lazy, vector
+    n = (1 << 30) + 5
+    kd = bench.device_uniform_u32(ex, 0, 0xFFFFFFFF, 21, n)
+    sel = bench.device_uniform_u32(ex, 0, 0xFFFFFFFF, 22, n)
+    k64 = kd.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    skew = (sel.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF) < int(0.6 * 2 ** 32)
+    k64 = torch.where(skew, (k64 & ~0xFF00) | 0x5A00, k64)
+    kd.tensor.view(torch.int32).copy_(k64.to(torch.int32))
+    del sel, skew, k64
+    vd = ex.alloc(np.uint32, n)
+    vector.copy(ex, lazy.counting(0).take(n), vd)
+    sk, sv = vector.radix_sort_pairs(ex, kd, vd)
+    ex.sync()
+    del vd
+    torch.cuda.empty_cache()
+    k = sk.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    v = sv.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    del sk, sv
+    kin = kd.tensor.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    assert torch.equal(kin[v], k), "output keys are not the input keys at the output values"
+    del kin
+    comp = k * (1 << 31) + v  # below 2^63: k < 2^32, v < 2^31
+    assert bool((comp[1:] > comp[:-1]).all()), "not sorted and stable"
+    del comp, k
+    seen = torch.zeros(n, dtype=torch.int8, device=v.device)
+    seen[v] = 1
+    assert bool(seen.all()), "values are not a permutation"

@@ -30,3 +30,30 @@ def test_corrupt_database_reads_as_empty(tmp_path):
     p = tmp_path / "db.json"
     p.write_text("{not json")
     assert tune.load_db(str(p)) == {}
+
+
+def test_database_lives_outside_the_package(monkeypatch, tmp_path):
+    import os
+
+    import massively_b200
+    monkeypatch.delenv("MB_TUNE_DB", raising=False)
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    p = tune.default_db_path()
+    assert p == os.path.join(str(tmp_path), "massively_b200", "tune_db.json")
+    pkg = os.path.dirname(os.path.abspath(massively_b200.__file__))
+    assert not os.path.abspath(p).startswith(pkg)
+    monkeypatch.setenv("MB_TUNE_DB", str(tmp_path / "x.json"))
+    assert tune.default_db_path() == str(tmp_path / "x.json")
+    tune.save_db({"k": {"config": 1}})  # creates the folder on demand
+    assert tune.load_db() == {"k": {"config": 1}}
+
+
+def test_segment_length_class_keys_records():
+    import numpy as np
+    even = tune.segment_class(np.full(1000, 64))
+    skew = tune.segment_class(np.random.default_rng(0).lognormal(3.0, 1.5, 1000))
+    assert even == "seg:mean2^6:cv0"
+    assert even != skew and skew.startswith("seg:")
+    assert tune.segment_class([]) == ""
+    assert tune._key("D", "seg", "f32", 1 << 26, even) == "D|seg|f32|2^26|seg:mean2^6:cv0"
+    assert tune._key("D", "radix", "u32", 1 << 26) == "D|radix|u32|2^26"
