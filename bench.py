@@ -821,8 +821,13 @@ def run_ours(args):
     import massively_b200 as mb
     ex = mb.Executor(local)
     from massively_b200 import tune
-    tune.apply(ex)  # persisted autotuner choices (or MB_TUNE_<FAMILY> overrides)
     wl = WORKLOADS[args.workload]()
+    # the autotuner's recorded choice for this workload's (dtype, n), or an
+    # MB_TUNE_<FAMILY> override, else the built-in default; reported below
+    chosen = tune.apply(ex, wl.dtype, wl.n)
+    tuning = {fam: {"config": c, "source": src,
+                    "describe": tune.configs(fam)[c] if c >= 0 else "built-in default"}
+              for fam, (c, src) in chosen.items()}
     wl.setup(ex)
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
@@ -863,6 +868,27 @@ def run_ours(args):
                 torch.cuda.empty_cache()
             except Exception as e:  # a secondary that is not built yet
                 secondary[name] = {"error": str(e)[:200]}
+        # the serving loop on a shortened trace (MB_SERVE_SECONDS s of arrivals)
+        try:
+            torch.cuda.empty_cache()
+            secs = float(os.environ.get("MB_SERVE_SECONDS", "1.0"))
+            m = serving_measure(ex, secs, 1, rank, local)
+            secondary["serving"] = {
+                "metric": "batched-request requests/s (p50/p99 latency)",
+                "value": m["ours"].req_per_s * world, "unit": "requests/s",
+                "trace": {**{k: v for k, v in m["cfg"].items() if k != "mix"},
+                          "mix": list(m["cfg"]["mix"]),
+                          "note": f"{secs:g} s of arrivals (the configuration's 10 s trace "
+                                  "shortened to keep the default run within minutes)"},
+                "p50_ms": m["ours"].p50_ms, "p99_ms": m["ours"].p99_ms,
+                "batched": _serve_stats(m["ours"]),
+                "plain_dispatch": _serve_stats(m["plain"]),
+                "queued_dispatch": _serve_stats(m["queued"]),
+                "speedup_requests_per_s": m["ours"].req_per_s / m["plain"].req_per_s,
+                "speedup_vs_queued": m["ours"].req_per_s / m["queued"].req_per_s,
+                "clocks": m["clocks"]}
+        except Exception as e:
+            secondary["serving"] = {"error": str(e)[:200]}
     e2e = None
     if not args.no_e2e:
         try:
@@ -881,7 +907,8 @@ def run_ours(args):
             "dtype": wl.dtype, "data": "synthetic (massively PCG streams, seeded)",
             "config": {"workload": wl.name, "items_per_gpu": wl.n,
                        "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (no flush needed)"},
+                       "l2": "inputs larger than L2 (no flush needed)",
+                       "tuning": tuning},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": NCU_TRAFFIC_BYTES.get(wl.name),
@@ -918,6 +945,36 @@ def gpu_launches(wl, steps):
     return per * steps
 
 
+def _serve_stats(st):
+    return {"requests_per_s": st.req_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+            "requests": st.requests, "launches": st.launches, "makespan_s": st.elapsed_s}
+
+
+def serving_measure(ex, secs, warmup, seed, device):
+    """The serving trace (Poisson 20k req/s for `secs` s of arrivals, mix
+    60/25/15, n log-uniform on [2^10, 2^26], 40 GB budget) through the
+    batched loop, awaited plain dispatch and queued plain dispatch, after a
+    short warm-up of both loops (kernels loaded, the stream-ordered pool
+    grown to its working size)."""
+    import torch
+
+    from massively_b200 import serving as S
+    cfg = dict(rate=20_000.0, duration=secs, lo_log2=10, hi_log2=26, mix=(0.60, 0.25, 0.15))
+    S.serve(ex, S.make_trace(**{**cfg, "duration": 0.1}, seed=99))
+    for _ in range(max(1, warmup)):
+        S.serve(ex, S.make_trace(**{**cfg, "duration": 0.01}, seed=98))
+        S.plain_dispatch(ex, S.make_trace(**{**cfg, "duration": 0.01}, seed=98), wait=False)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(device)
+    sampler.start()
+    ours = S.serve(ex, S.make_trace(**cfg, seed=seed))
+    plain = S.plain_dispatch(ex, S.make_trace(**cfg, seed=seed), wait=True)
+    queued = S.plain_dispatch(ex, S.make_trace(**cfg, seed=seed), wait=False)
+    clocks = sampler.stop()
+    ex.sync()
+    return {"ours": ours, "plain": plain, "queued": queued, "clocks": clocks, "cfg": cfg}
+
+
 def run_serving(args):
     """The batched request loop against plain one-request-per-launch
     dispatch on the same seeded trace: Poisson arrivals at 20k req/s, mix
@@ -929,34 +986,16 @@ def run_serving(args):
     import torch
 
     import massively_b200 as mb
-    from massively_b200 import serving as S
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     ex = mb.Executor(local)
     secs = float(os.environ.get("MB_SERVE_SECONDS", "1.0"))
-    cfg = dict(rate=20_000.0, duration=secs, lo_log2=10, hi_log2=26, mix=(0.60, 0.25, 0.15))
-    # warm-up: a 0.1 s trace of the same distribution through both loops
-    # (loads the kernels and grows the stream-ordered pool to its working
-    # size, so no timed loop pays for the pool's first growth)
-    S.serve(ex, S.make_trace(**{**cfg, "duration": 0.1}, seed=99))
-    for _ in range(max(1, args.warmup)):
-        S.serve(ex, S.make_trace(**{**cfg, "duration": 0.01}, seed=98))
-        S.plain_dispatch(ex, S.make_trace(**{**cfg, "duration": 0.01}, seed=98), wait=False)
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    ours = S.serve(ex, S.make_trace(**cfg, seed=rank))
-    plain = S.plain_dispatch(ex, S.make_trace(**cfg, seed=rank), wait=True)
-    queued = S.plain_dispatch(ex, S.make_trace(**cfg, seed=rank), wait=False)
-    clocks = sampler.stop()
-    ex.sync()
+    m = serving_measure(ex, secs, args.warmup, rank, local)
+    ours, plain, queued, clocks, cfg = m["ours"], m["plain"], m["queued"], m["clocks"], m["cfg"]
     if rank == 0:
-        def d(st):
-            return {"requests_per_s": st.req_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
-                    "requests": st.requests, "launches": st.launches,
-                    "makespan_s": st.elapsed_s}
+        d = _serve_stats
         line = {
             "metric": "batched-request requests/s (p50/p99 latency)",
             "value": ours.req_per_s * world, "unit": "requests/s", "n_gpus": world,

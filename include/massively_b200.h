@@ -588,6 +588,19 @@ int mb_inclusive_scan_user(mb_executor* exec, const mb_src* in, mb_user_op* op, 
 int mb_exclusive_scan_user(mb_executor* exec, const mb_src* in, mb_user_op* op, const void* init,
                            mb_col out);
 int mb_map_user(mb_executor* exec, const mb_src* in, mb_user_op* op, mb_col out);
+/* A user comparator (massively `op::BinaryPredicateOp`, core/ordering/
+ * mod.rs:53-56): `source` defines `__device__ bool name(T a, T b)`, a strict
+ * weak order ("a before b").  mb_sort_user is vector::sort / sort_by_key
+ * under it (massively/src/api/algorithm/ordering.rs:64-76, by_key.rs:
+ * 226-270; core massively/src/core/ordering/sort.rs:54-455): a stable merge
+ * sort of a plain key column of the compiled type, writing the sorted keys
+ * (when out_keys.data is non-NULL) and the `nvals` (0..12) value columns
+ * permuted alike; ties keep their input order.  mb_user_op_check takes kind
+ * 2 for a comparator. */
+int mb_user_pred_compile(mb_executor* exec, int dtype, const char* source, const char* name,
+                         mb_user_op** out);
+int mb_sort_user(mb_executor* exec, const mb_src* keys, mb_user_op* less, const mb_src* values,
+                 int nvals, mb_col out_keys, const mb_col* out_values);
 
 /* ------------------------------------------------------- kernel timing ---- */
 

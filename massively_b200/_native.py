@@ -97,6 +97,8 @@ def _declare(L: C.CDLL) -> None:
         "mb_user_op_compile": (i32, [vp, i32, C.c_char_p, C.c_char_p, _P(vp)]),
         "mb_user_map_compile": (i32, [vp, i32, i32, C.c_char_p, C.c_char_p, _P(vp)]),
         "mb_user_op_check": (i32, [i32, i32, i32, C.c_char_p, C.c_char_p]),
+        "mb_user_pred_compile": (i32, [vp, i32, C.c_char_p, C.c_char_p, _P(vp)]),
+        "mb_sort_user": (i32, [vp, src, vp, src, i32, col, pcol]),
         "mb_user_op_destroy": (i32, [vp]),
         "mb_reduce_user": (i32, [vp, src, vp, vp, vp, vp]),
         "mb_inclusive_scan_user": (i32, [vp, src, vp, col]),

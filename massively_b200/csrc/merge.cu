@@ -281,7 +281,7 @@ __device__ __forceinline__ void set_block_scans(int& a, int& b, int& c, int& d, 
 
 // MODE: 0 union, 1 intersection, 2 difference.
 template <class T, int LESS, bool PLAIN>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     set_tile_kernel(int MODE, Src L, Src R, void* out, int out_esize, uint32_t* count_dev,
                     const uint64_t* __restrict__ splits, const SetRun* __restrict__ runs,
                     const T* __restrict__ vals, uint32_t* counter, TileState<uint32_t, true> st,
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ uint8_t s_right[kTile];
   __shared__ int s_tmp[4 * (kThreads / 32)];
   __shared__ uint32_t s_wcount[kThreads / 32];
-  __shared__ uint32_t s_tile, s_excl;
+  __shared__ uint32_t s_tile, s_excl, s_tile_kept;
   __shared__ uint64_t s_split[2];
   const uint64_t nl = src_len(L), nr = src_len(R), n = nl + nr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -408,30 +408,31 @@ __global__ void __launch_bounds__(kThreads)
   for (int k = 0; k < kItems; ++k) {
     keep[k] = false;
     if (k >= cnt) continue;
-    const uint64_t g = d0 + dt + k;
-    uint64_t grs, glr, gre;
     const bool use0 = first_open && rs[k] == 0;
     const bool use1 = !use0 && last_open && rs[k] == last_rs;
-    if (use0 || use1) {
-      const SetRun x = use0 ? r0 : r1;
-      grs = (uint64_t)x.lbl + x.lbr;
-      glr = grs + (x.ubl - x.lbl);
-      gre = (uint64_t)x.ubl + x.ubr;
-    } else {
-      const int e = re[k] == kNone ? total : re[k];
-      int lr;
-      if (!right[k]) lr = min(rr[k] == kNone ? total : rr[k], e);
-      else lr = max(ll[k] + 1, rs[k]);
-      grs = d0 + rs[k];
-      glr = d0 + lr;
-      gre = d0 + e;
-    }
     bool kp;
-    if (!right[k]) {
-      const uint64_t rank = g - grs, other = gre - glr;
-      kp = MODE == 0 ? true : MODE == 1 ? rank < other : rank >= other;
-    } else {
-      kp = MODE == 0 && (g - glr) >= (glr - grs);
+    if (use0 || use1) {  // a run crossing the tile's edge: global positions
+      const SetRun x = use0 ? r0 : r1;
+      const uint64_t g = d0 + dt + k;
+      const uint64_t grs = (uint64_t)x.lbl + x.lbr;
+      const uint64_t cl = x.ubl - x.lbl, cr = x.ubr - x.lbr;
+      if (!right[k]) {
+        const uint64_t rank = g - grs;
+        kp = MODE == 0 || (MODE == 1 ? rank < cr : rank >= cr);
+      } else {
+        kp = MODE == 0 && g - (grs + cl) >= cl;
+      }
+    } else {  // a run inside the tile: tile positions
+      const int t = dt + k;
+      const int e = re[k] == kNone ? total : re[k];
+      if (!right[k]) {
+        const int lr = min(rr[k] == kNone ? total : rr[k], e);
+        const int rank = t - rs[k], cr = e - lr;
+        kp = MODE == 0 || (MODE == 1 ? rank < cr : rank >= cr);
+      } else {
+        const int lr = max(ll[k] + 1, rs[k]);
+        kp = MODE == 0 && t - lr >= lr - rs[k];
+      }
     }
     keep[k] = kp;
     kept += kp ? 1u : 0u;
@@ -461,19 +462,24 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (lane == 0) {
       s_excl = excl;
+      s_tile_kept = agg;
       if (d1 == n && count_dev) *count_dev = excl + agg;
     }
   }
-  __syncthreads();
-  uint32_t pos = s_excl + incl - kept;
-  for (int w = 0; w < warp; ++w) pos += s_wcount[w];
-  const uint64_t cap = MODE == 0 ? n : nl;
+  // The kept items, compacted in tile order into s_keys (free since the
+  // merge), then written with consecutive threads on consecutive addresses.
+  uint32_t lpos = incl - kept;
+  for (int w = 0; w < warp; ++w) lpos += s_wcount[w];
 #pragma unroll
-  for (int k = 0; k < kItems; ++k) {
-    if (!keep[k]) continue;
-    if (pos < cap) st_raw_pay(out, pos, out_esize, to_bits64(s_out[dt + k]));
+  for (int k = 0; k < kItems; ++k)
+    if (keep[k]) s_keys[lpos++] = s_out[dt + k];
+  __syncthreads();
+  const uint64_t base = s_excl;
+  const uint32_t tile_kept = s_tile_kept;
+  const uint64_t cap = MODE == 0 ? n : nl;
+  for (uint32_t i = tid; i < tile_kept; i += kThreads) {
+    if (base + i < cap) st_raw_pay(out, base + i, out_esize, to_bits64(s_keys[i]));
     else raise_device_error(err, MB_DEV_ERR_BOUNDS);  // only after a failed look-back
-    ++pos;
   }
 }
 

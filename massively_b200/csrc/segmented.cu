@@ -46,7 +46,19 @@ constexpr int kSegMinBlocks = 4;
 // look-back -- each tile reduces the segments that start and end in it and
 // leaves two partial folds for the segments that cross its edges, which
 // seg_reduce_cross_kernel then folds in tile order.
-enum SegMode : int { kScanIncl = 0, kScanExcl = 1, kReduce = 2, kReduceTiles = 3 };
+// kScanInclTiles / kScanExclTiles: the segmented scans over offsets without
+// the look-back -- every tile scans as if it started a segment and leaves
+// its tail fold; seg_tile_carry_kernel scans those folds over the tiles
+// (a segmented scan of one value per tile), and seg_scan_fix_kernel applies
+// each tile's carry to the items before its first segment start.
+enum SegMode : int {
+  kScanIncl = 0,
+  kScanExcl = 1,
+  kReduce = 2,
+  kReduceTiles = 3,
+  kScanInclTiles = 4,
+  kScanExclTiles = 5
+};
 enum HeadsSrc : int { kHeadsOffsets = 0, kHeadsKeys = 1 };
 
 template <class V>
@@ -198,19 +210,47 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   const uint64_t te = min(tb + (uint64_t)C::TILE, n);
   const bool last_tile = te == n;
 
+  // ---- value loads, issued first so their latency overlaps the heads ----
+  const SegOp<V, OP> op{Op<V, OP>{p.op}};
+  const int warp = tid >> 5, lane = tid & 31;
+  const uint64_t warp_base = tb + (uint64_t)warp * C::WARP_ITEMS;
+  const bool full = tb + C::TILE <= n;
+  V raw[kLoads][VEC];
+  if (PLAIN && full) {
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      uint4 u = __ldcs(reinterpret_cast<const uint4*>((const V*)in.data + warp_base +
+                                                      (uint64_t)(j * 32 + lane) * VEC));
+      memcpy(raw[j], &u, 16);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) {
+        const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
+        if (i < n) {
+          if constexpr (PLAIN) raw[j][k] = ((const V*)in.data)[i];
+          else raw[j][k] = src_load<V>(in, i);
+        } else {
+          raw[j][k] = V(0);
+        }
+      }
+  }
+
   // ---- heads ----
   if (p.heads_src == kHeadsOffsets) {
+    // Every thread reads the tile's segment range (broadcast loads).
+    const uint64_t sa = p.tile_lb[tile];  // first start >= tb
+    const uint64_t sb = last_tile ? p.nseg : min((uint64_t)p.tile_lb[tile + 1], p.nseg);
     if (tid == 0) {
-      const uint64_t sa = p.tile_lb[tile];  // first start >= tb
-      const uint64_t sb = last_tile ? p.nseg : min((uint64_t)p.tile_lb[tile + 1], p.nseg);
       // The segment before sa holds tb (and continues into this tile)
       // unless one starts exactly at tb.
       s_seg[0] = (sa > 0 && p.offsets[sa] > tb) ? sa - 1 : ~0ull;
       s_seg[1] = sa;
       s_seg[2] = sb;
     }
-    __syncthreads();
-    for (uint64_t s = s_seg[1] + tid; s < s_seg[2]; s += kThreads) {
+    for (uint64_t s = sa + tid; s < sb; s += kThreads) {
       const uint64_t start = p.offsets[s];
       if (start >= tb && start < te) atomicOr(&s_bits[(start - tb) >> 5], 1u << ((start - tb) & 31));
     }
@@ -246,44 +286,16 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   }
   __syncthreads();
 
-  // ---- load (value, head) pairs ----
-  const SegOp<V, OP> op{Op<V, OP>{p.op}};
-  const int warp = tid >> 5, lane = tid & 31;
-  const uint64_t warp_base = tb + (uint64_t)warp * C::WARP_ITEMS;
-  const bool full = tb + C::TILE <= n;
+  // ---- (value, head) pairs ----
   T x[kLoads][VEC];
-  {
-    V raw[kLoads][VEC];
-    if (PLAIN && full) {
 #pragma unroll
-      for (int j = 0; j < kLoads; ++j) {
-        uint4 u = __ldcs(reinterpret_cast<const uint4*>((const V*)in.data +
-                                                        warp_base + (uint64_t)(j * 32 + lane) * VEC));
-        memcpy(raw[j], &u, 16);
-      }
-    } else {
+  for (int j = 0; j < kLoads; ++j)
 #pragma unroll
-      for (int j = 0; j < kLoads; ++j)
-#pragma unroll
-        for (int k = 0; k < VEC; ++k) {
-          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
-          if (i < n) {
-            if constexpr (PLAIN) raw[j][k] = ((const V*)in.data)[i];
-            else raw[j][k] = src_load<V>(in, i);
-          } else {
-            raw[j][k] = V(0);
-          }
-        }
+    for (int k = 0; k < VEC; ++k) {
+      const uint32_t pos = (uint32_t)(warp_base - tb) + (j * 32 + lane) * VEC + k;
+      x[j][k].v = raw[j][k];
+      x[j][k].heads = (s_bits[pos >> 5] >> (pos & 31)) & 1u;
     }
-#pragma unroll
-    for (int j = 0; j < kLoads; ++j)
-#pragma unroll
-      for (int k = 0; k < VEC; ++k) {
-        const uint32_t pos = (uint32_t)(warp_base - tb) + (j * 32 + lane) * VEC + k;
-        x[j][k].v = raw[j][k];
-        x[j][k].heads = (s_bits[pos >> 5] >> (pos & 31)) & 1u;
-      }
-  }
 
   // ---- tile scan (same structure as the plain scan kernel) ----
 #pragma unroll
@@ -308,7 +320,8 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   for (int j = 1; j < kLoads; ++j) rp[j] = op(rp[j - 1], rowtot[j]);
   if (lane == 0) s_warp_total[warp] = rp[kLoads - 1];
   __syncthreads();
-  const bool local = p.mode == kReduceTiles;  // no look-back: every tile starts fresh
+  // no look-back: every tile starts fresh
+  const bool local = p.mode == kReduceTiles || p.mode >= kScanInclTiles;
   if (warp == 0 && !local) {
     T agg = s_warp_total[0];
 #pragma unroll
@@ -347,9 +360,9 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   }
 
   const Op<V, OP> vop{p.op};
-  if (p.mode == kScanIncl || p.mode == kScanExcl) {
+  if (p.mode == kScanIncl || p.mode == kScanExcl || p.mode >= kScanInclTiles) {
     V o[kLoads][VEC];
-    if (p.mode == kScanIncl) {
+    if (p.mode == kScanIncl || p.mode == kScanInclTiles) {
 #pragma unroll
       for (int j = 0; j < kLoads; ++j)
 #pragma unroll
@@ -367,9 +380,22 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
           const uint32_t pos = (uint32_t)(warp_base - tb) + (j * 32 + lane) * VEC + k;
           const bool hd = ((s_bits[pos >> 5] >> (pos & 31)) & 1u) || tb + pos == 0;
           const V prev = k == 0 ? prev0 : y[j][k - 1].v;
-          o[j][k] = hd ? p.init : vop(p.init, prev);
+          // (without the look-back, the items of a segment that came in from
+          // an earlier tile keep their tile-local inclusive value here;
+          // seg_scan_fix_kernel turns it into the exclusive result)
+          o[j][k] = local && y[j][k].heads == 0 ? y[j][k].v
+                                                : (hd ? p.init : vop(p.init, prev));
         }
       }
+    }
+    if (local) {  // the tile's tail fold, for the carries of later tiles
+#pragma unroll
+      for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          const uint64_t i = warp_base + (uint64_t)(j * 32 + lane) * VEC + k;
+          if (i + 1 == te) p.part_tail[tile] = y[j][k].v;
+        }
     }
     if (PLAIN && full && p.out_dtype == DTypeOf<V>::value) {
 #pragma unroll
@@ -391,6 +417,11 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   }
 
   // ---- reductions: stage inclusive pairs, write one value per tail ----
+  // (kReduceTiles: the segments that start and end in this tile are written
+  // here; the tile leaves its fold before its first segment start, its fold
+  // from its last start to its end, and the segment that starts there when it
+  // goes on past the tile, for seg_reduce_cross_kernel.  Writing by segment
+  // index keeps the per-segment stores coalesced.)
 #pragma unroll
   for (int j = 0; j < kLoads; ++j)
 #pragma unroll
@@ -408,9 +439,7 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
         if ((start >= tb && start < te) || (last_tile && start >= te))
           st_cast<V>(p.out_dtype, p.out, s, p.init);
       } else if (end - 1 >= tb && end - 1 < te) {
-        // (kReduceTiles: a segment that started in an earlier tile is
-        // finished by seg_reduce_cross_kernel)
-        if (!local || start >= tb)
+        if (!local || start >= tb)  // else: finished by seg_reduce_cross_kernel
           st_cast<V>(p.out_dtype, p.out, s, vop(p.init, stage[end - 1 - tb].v));
       } else if (local && start >= tb && start < te) {
         p.tail_seg[tile] = (uint32_t)s;  // goes on past this tile
@@ -419,9 +448,7 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
     if (tid == 0 && s_seg[0] != ~0ull) write_seg(s_seg[0]);
     for (uint64_t s = s_seg[1] + tid; s < s_seg[2]; s += kThreads) write_seg(s);
     if (local) {
-      // The fold before the first segment start (the whole tile when none
-      // starts in it) and the fold from the last start to the tile's end.
-      __shared__ uint32_t s_first;
+      __shared__ uint32_t s_first;  // the tile's first segment start
       if (tid == 0) s_first = (uint32_t)(te - tb);
       __syncthreads();
       if (tid < C::TILE / 32 && s_bits[tid])
@@ -479,6 +506,125 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Whether tile t (items [t * tile_items, te)) holds a segment start: the
+// first start at or after its beginning lies before its end.
+__device__ __forceinline__ bool tile_has_start(const uint32_t* offsets, const uint32_t* tile_lb,
+                                               uint64_t t, uint64_t te) {
+  return (uint64_t)offsets[tile_lb[t]] < te;
+}
+
+constexpr int kCarryThreads = 1024;
+
+// kScan*Tiles: carry[t] = the fold of the segment that enters tile t over
+// the items before t -- the value of an inclusive segmented scan, over the
+// tiles, of (tile holds a start, its tail fold) at tile t - 1.  One block;
+// each thread folds a contiguous run of tiles, a block scan (fixed shape)
+// joins the runs, and the threads walk their runs again, so the result is
+// the same from run to run.
+template <class V>
+__global__ void __launch_bounds__(kCarryThreads)
+    seg_tile_carry_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ tile_lb,
+                          uint64_t tiles, uint64_t tile_items, uint64_t cap,
+                          const uint32_t* __restrict__ n_dev, int op,
+                          const V* __restrict__ part_tail, V* __restrict__ carry) {
+  using T = SegVal<V>;
+  const SegOp<V, kOpDyn> sop{Op<V, kOpDyn>{op}};
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t live = (n + tile_items - 1) / tile_items < tiles ? (n + tile_items - 1) / tile_items
+                                                                  : tiles;
+  const uint64_t per = (live + kCarryThreads - 1) / kCarryThreads;
+  const uint64_t u0 = threadIdx.x * per, u1 = min(u0 + per, live);
+  auto item = [&](uint64_t u) -> T {
+    const uint64_t te = min((u + 1) * tile_items, n);
+    return T{tile_has_start(offsets, tile_lb, u, te) ? 1u : 0u, part_tail[u]};
+  };
+  T agg{0, V(0)};
+  bool has = false;
+  for (uint64_t u = u0; u < u1; ++u) {
+    const T x = item(u);
+    agg = has ? sop(agg, x) : x;
+    has = true;
+  }
+  __shared__ T s_v[kCarryThreads];
+  __shared__ int s_h[kCarryThreads];
+  s_v[threadIdx.x] = agg;
+  s_h[threadIdx.x] = has;
+  __syncthreads();
+  for (int d = 1; d < kCarryThreads; d <<= 1) {  // inclusive, in thread order
+    T x{};
+    int hx = 0;
+    if (threadIdx.x >= d && s_h[threadIdx.x - d]) {
+      x = s_h[threadIdx.x] ? sop(s_v[threadIdx.x - d], s_v[threadIdx.x]) : s_v[threadIdx.x - d];
+      hx = 1;
+    }
+    __syncthreads();
+    if (hx) {
+      s_v[threadIdx.x] = x;
+      s_h[threadIdx.x] = 1;
+    }
+    __syncthreads();
+  }
+  T run{0, V(0)};
+  bool rh = threadIdx.x > 0 && s_h[threadIdx.x - 1];
+  if (rh) run = s_v[threadIdx.x - 1];
+  for (uint64_t u = u0; u < u1; ++u) {
+    if (rh) carry[u] = run.v;
+    const T x = item(u);
+    run = rh ? sop(run, x) : x;
+    rh = true;
+  }
+}
+
+// kScan*Tiles: the items of tile t before its first segment start belong to
+// a segment that began in an earlier tile; the tile kernel left their
+// tile-local inclusive values in `out`.  Inclusive: carry op local;
+// exclusive: init op (carry op local of the item before), init op carry for
+// the tile's first item.  All loads come before the barrier, all stores
+// after it.
+template <class V>
+__global__ void __launch_bounds__(kThreads)
+    seg_scan_fix_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ tile_lb,
+                        uint64_t tile_items, uint64_t cap, const uint32_t* __restrict__ n_dev,
+                        int op, int exclusive, V init, const V* __restrict__ carry, void* out,
+                        int out_dtype) {
+  constexpr int MAXR = (int)(SegCfg<V>::TILE / kThreads);
+  const uint64_t t = blockIdx.x + 1;  // tile 0 starts with a segment
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t tb = t * tile_items;
+  if (tb >= n) return;
+  const uint64_t te = min(tb + tile_items, n);
+  const uint64_t first = min((uint64_t)offsets[tile_lb[t]], te);
+  if (first == tb) return;
+  const uint64_t len = first - tb;
+  const V c = carry[t];
+  Src o{};
+  o.kind = MB_SRC_COLUMN;
+  o.dtype = out_dtype;
+  o.vtype = DTypeOf<V>::value;
+  o.map = MB_UN_IDENTITY;
+  o.data = out;
+  o.len = cap;
+  V x[MAXR], xp[MAXR];
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) {
+    const uint64_t i = (uint64_t)r * kThreads + threadIdx.x;
+    if (i < len) {
+      x[r] = src_load<V>(o, tb + i);
+      if (exclusive && i > 0) xp[r] = src_load<V>(o, tb + i - 1);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) {
+    const uint64_t i = (uint64_t)r * kThreads + threadIdx.x;
+    if (i >= len) continue;
+    V v;
+    if (!exclusive) v = op_apply_rt<V>(op, c, x[r]);
+    else v = op_apply_rt<V>(op, init, i == 0 ? c : op_apply_rt<V>(op, c, xp[r]));
+    st_cast<V>(out_dtype, out, tb + i, v);
+  }
+}
+
 template <class V>
 int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_wide) {
   using C = SegCfg<V>;
@@ -492,7 +638,10 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   const size_t state_b =
       pk ? TileState<T, true>::bytes(tiles) : TileState<T, false>::bytes(tiles);
   const size_t lb_b = p.offsets ? ((tiles + 1) * 4 + 255) / 256 * 256 : 0;
-  const bool tiles_mode = p.mode == kReduceTiles;
+  // kReduceTiles: part_head, part_tail, tail_seg; kScan*Tiles: part_tail and
+  // the carries (in the part_head slot).
+  const bool scan_tiles = p.mode >= kScanInclTiles;
+  const bool tiles_mode = p.mode == kReduceTiles || scan_tiles;
   const size_t part_b = tiles_mode ? (tiles * sizeof(V) + 255) / 256 * 256 : 0;
   const size_t tseg_b = tiles_mode ? (tiles * 4 + 255) / 256 * 256 : 0;
   Scratch scratch;
@@ -517,7 +666,8 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
     p.tile_lb = lb;
   }
   const bool plain = src_plain(in, DTypeOf<V>::value) && (uintptr_t)in.data % 16 == 0 &&
-                     (p.mode >= kReduce || (uintptr_t)p.out % 16 == 0);
+                     (p.mode == kReduce || p.mode == kReduceTiles ||
+                      (uintptr_t)p.out % 16 == 0);
   const Src s = to_src(in);
   const size_t smem = seg_smem<V>(p.mode);
   char* state_base = scratch.as<char>() + 256;
@@ -549,7 +699,17 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   }
 #undef MB_SEG_LAUNCH
   MB_CUDA(cudaGetLastError());
-  if (tiles_mode) {
+  if (scan_tiles) {
+    seg_tile_carry_kernel<V><<<1, kCarryThreads, 0, ex->stream>>>(
+        p.offsets, p.tile_lb, tiles, C::TILE, cap, in.len_dev, p.op, p.part_tail, p.part_head);
+    MB_CUDA(cudaGetLastError());
+    if (tiles > 1) {
+      seg_scan_fix_kernel<V><<<(unsigned)(tiles - 1), kThreads, 0, ex->stream>>>(
+          p.offsets, p.tile_lb, C::TILE, cap, in.len_dev, p.op,
+          p.mode == kScanExclTiles ? 1 : 0, p.init, p.part_head, p.out, p.out_dtype);
+      MB_CUDA(cudaGetLastError());
+    }
+  } else if (tiles_mode) {
     const unsigned g = (unsigned)std::min<uint64_t>((tiles + kThreads - 1) / kThreads, 4096);
     seg_reduce_cross_kernel<V><<<std::max(1u, g), kThreads, 0, ex->stream>>>(
         p.offsets, tiles, C::TILE, p.op, p.init, p.part_head, p.part_tail, p.tail_seg, p.out,
@@ -914,15 +1074,18 @@ int mb_segmentation_from_segment_ids(mb_executor* ex, const mb_src* ids, uint64_
 int mb_seg_inclusive_scan(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
                           uint64_t segment_count, int op, mb_col out) {
   MB_TRY(check_values_out(ex, values, out, values ? values->len : 0));
-  return seg_entry(ex, values, op, kScanIncl, nullptr, out.data, out.dtype, offsets,
-                   segment_count, nullptr, nullptr, 0, nullptr);
+  // MB_TUNE_SEG: 0 = tile-local scans plus carries (default), 1 = look-back
+  const int mode = ex->tune[MB_TUNE_SEG] == 1 ? kScanIncl : kScanInclTiles;
+  return seg_entry(ex, values, op, mode, nullptr, out.data, out.dtype, offsets, segment_count,
+                   nullptr, nullptr, 0, nullptr);
 }
 
 int mb_seg_exclusive_scan(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
                           uint64_t segment_count, int op, const void* init, mb_col out) {
   MB_TRY(check_values_out(ex, values, out, values ? values->len : 0));
   if (!init) return set_error(MB_ERR_LAUNCH, "exclusive scan needs an init value");
-  return seg_entry(ex, values, op, kScanExcl, init, out.data, out.dtype, offsets, segment_count,
+  const int mode = ex->tune[MB_TUNE_SEG] == 1 ? kScanExcl : kScanExclTiles;
+  return seg_entry(ex, values, op, mode, init, out.data, out.dtype, offsets, segment_count,
                    nullptr, nullptr, 0, nullptr);
 }
 

@@ -60,10 +60,13 @@ __device__ __forceinline__ void st_raw(void* p, uint64_t i, int esize, uint64_t 
   }
 }
 
-// FAST: one plain 4-byte column, flags fused on it or a plain u32 stencil.
-template <bool FAST>
+// NC > 0: NC plain 4-byte columns (all of them), flags fused on column 0 or
+// a plain u32 stencil; every column's items are loaded before the look-back,
+// so their latency overlaps it.  NC = 0: any columns and views, loaded after.
+template <int NC>
 __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t cap,
                                                           TileState<uint32_t, true> st) {
+  constexpr bool FAST = NC > 0;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_wcount[kWarps];
   __shared__ uint32_t s_excl;
@@ -77,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
   const uint64_t warp_base = tile_base + (uint64_t)warp * 32 * kItems;
   const uint32_t invert = p.mode == kRemove ? 1u : 0u;
 
-  uint32_t v0[FAST ? kItems : 1];
+  uint32_t v[FAST ? NC : 1][FAST ? kItems : 1];
   unsigned ballot[kItems];
   uint32_t wcount = 0;
 #pragma unroll
@@ -87,8 +90,9 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
     uint32_t f = 0;
     if (valid) {
       if constexpr (FAST) {
-        v0[k] = __ldcs((const uint32_t*)p.cols[0].data + i);
-        if (p.fused) f = map_to<uint32_t>(p.fused_map, p.cols[0].dtype, v0[k]) != 0;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) v[c][k] = __ldcs((const uint32_t*)p.cols[c].data + i);
+        if (p.fused) f = map_to<uint32_t>(p.fused_map, p.cols[0].dtype, v[0][k]) != 0;
         else f = __ldcs((const uint32_t*)p.stencil.data + i) != 0;
       } else {
         f = src_load<uint32_t>(p.stencil, i) != 0;
@@ -138,10 +142,13 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
     run += __popc(ballot[k]);
   }
   if constexpr (FAST) {
-    uint32_t* out = (uint32_t*)p.outs[0];
 #pragma unroll
-    for (int k = 0; k < kItems; ++k)
-      if (pos[k] != 0xFFFFFFFFu) out[pos[k]] = v0[k];
+    for (int c = 0; c < NC; ++c) {
+      uint32_t* out = (uint32_t*)p.outs[c];
+#pragma unroll
+      for (int k = 0; k < kItems; ++k)
+        if (pos[k] != 0xFFFFFFFFu) out[pos[k]] = v[c][k];
+    }
   } else {
     for (int c = 0; c < p.ncols; ++c) {
 #pragma unroll 4
@@ -328,10 +335,15 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
                            in[0].map == MB_UN_IDENTITY;
     p.fused = same_data && stencil->map != MB_UN_IDENTITY;
     p.fused_map = stencil->map;
-    const bool fast = ncols == 1 && src_plain(in[0], in[0].vtype) &&
-                      dtype_size(in[0].vtype) == 4 && in[0].len_dev == nullptr &&
-                      (p.fused || (src_plain(*stencil, MB_U32) && stencil->vtype == MB_U32 &&
-                                   stencil->dtype == MB_U32 && stencil->len_dev == nullptr));
+    // Every column plain, 4 bytes wide, without a device length; the flags
+    // fused on column 0 or a plain u32 stencil.
+    bool plain4 = ncols <= 3 &&
+                  (p.fused || (src_plain(*stencil, MB_U32) && stencil->vtype == MB_U32 &&
+                               stencil->dtype == MB_U32 && stencil->len_dev == nullptr));
+    for (int c = 0; c < ncols && plain4; ++c)
+      plain4 = src_plain(in[c], in[c].vtype) && dtype_size(in[c].vtype) == 4 &&
+               in[c].len_dev == nullptr;
+    const bool fast = ncols == 1 && plain4;
     const uint64_t tiles = (n + kTile - 1) / kTile;
     Scratch scratch;
     MB_TRY(scratch.alloc(ex, 256 + tiles * 8));
@@ -365,10 +377,15 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
       else if (int4 && stencil->map == MB_UN_IS_FALSE)
         MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_FALSE>));
       else MB_TRY(launch(select_smem_kernel<true, -1>));
-    } else if (fast)
-      select_kernel<true><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
-    else
-      select_kernel<false><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    } else if (fast) {
+      select_kernel<1><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    } else if (plain4 && ncols == 2) {
+      select_kernel<2><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    } else if (plain4 && ncols == 3) {
+      select_kernel<3><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    } else {
+      select_kernel<0><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
+    }
     MB_CUDA(cudaGetLastError());
   }
   if (count_host) MB_TRY(read_u32(ex, count_dev, count_host));

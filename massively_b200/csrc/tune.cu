@@ -30,9 +30,10 @@ const char* mb_tune_describe(int family, int config) {
   if (family == MB_TUNE_SCAN && config == 2)
     return "scan one 64 KB tile per CTA, a ninth warp runs the look-back";
   if (family == MB_TUNE_SEG && config == 0)
-    return "segmented reduce: tile-local folds, then one pass over the segments crossing tiles";
+    return "segmented scan / reduce over offsets: tile-local work, then the carries of the "
+           "segments crossing tiles";
   if (family == MB_TUNE_SEG && config == 1)
-    return "segmented reduce: the segmented scan with its look-back carried across tiles";
+    return "segmented scan / reduce over offsets: a decoupled look-back carried across tiles";
   if (config == 0) {
     switch (family) {
       case MB_TUNE_SCAN: return "scan one 32 KB tile per CTA, a ninth warp runs the look-back";

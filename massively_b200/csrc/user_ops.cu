@@ -231,6 +231,141 @@ extern "C" __global__ void mbj_scan_apply(const T* loc, T* out, unsigned long lo
 }
 )MBJ";
 
+// Stable merge sort of (key, index) pairs under USER_LESS(a, b) -- massively's
+// comparator sort (core/ordering/sort.rs:54-455: block sorts, then merge
+// passes; ties keep input order).  Tiles of MBS_TILE items are sorted in
+// shared memory (each thread's 4 items by insertion, then pairwise merges of
+// doubling runs); the merge passes then merge runs of width w into 2w, each
+// block producing one tile of the output: its merge-path split in the two
+// runs (a binary search in global memory), both slices staged in shared
+// memory, each thread merging 4 outputs.  A merge takes the left item unless
+// the right one is strictly less, so equal keys keep their input order.
+const char* kSortKernels = R"MBJ(
+#define MBS_THREADS 256
+#define MBS_ITEMS 4
+#define MBS_TILE (MBS_THREADS * MBS_ITEMS)
+// Items of the merge of a[0, la) and b[0, lb) before output position d that
+// come from a (the merge-path split).
+template <class K>
+__device__ __forceinline__ int mbs_split(const K* a, int la, const K* b, int lb, int d) {
+  int lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (!USER_LESS(b[d - 1 - mid], a[mid])) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+// Serial merge of `cnt` outputs starting at split (i, j).
+template <class K>
+__device__ __forceinline__ void mbs_merge_out(const K* ka, const unsigned* ia, int la,
+                                              const K* kb, const unsigned* ib, int lb, int i,
+                                              int j, int cnt, K* ko, unsigned* io) {
+  for (int c = 0; c < cnt; ++c) {
+    const bool left = j >= lb || (i < la && !USER_LESS(kb[j], ka[i]));
+    if (left) { ko[c] = ka[i]; io[c] = ia[i]; ++i; }
+    else { ko[c] = kb[j]; io[c] = ib[j]; ++j; }
+  }
+}
+// Sorts each tile; idx = the input position of every key.
+extern "C" __global__ void mbs_block_sort(const T* keys, unsigned long long n, T* out_k,
+                                          unsigned* out_i) {
+  __shared__ T sk[2][MBS_TILE];
+  __shared__ unsigned si[2][MBS_TILE];
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * MBS_TILE;
+  const int cnt = (int)(n - t0 < MBS_TILE ? n - t0 : MBS_TILE);
+  const int base = threadIdx.x * MBS_ITEMS;
+  T k[MBS_ITEMS];
+  unsigned ix[MBS_ITEMS];
+  int mine = cnt - base;
+  mine = mine < 0 ? 0 : (mine > MBS_ITEMS ? MBS_ITEMS : mine);
+  for (int q = 0; q < mine; ++q) { k[q] = keys[t0 + base + q]; ix[q] = (unsigned)(t0 + base + q); }
+  for (int q = 1; q < mine; ++q) {  // stable insertion sort of the thread's items
+    T x = k[q];
+    unsigned y = ix[q];
+    int r = q - 1;
+    while (r >= 0 && USER_LESS(x, k[r])) { k[r + 1] = k[r]; ix[r + 1] = ix[r]; --r; }
+    k[r + 1] = x;
+    ix[r + 1] = y;
+  }
+  for (int q = 0; q < mine; ++q) { sk[0][base + q] = k[q]; si[0][base + q] = ix[q]; }
+  __syncthreads();
+  int src = 0;
+  for (int w = MBS_ITEMS; w < MBS_TILE; w <<= 1) {
+    // merge runs [a, a + w) and [a + w, a + 2w) (clipped to cnt)
+    const int pair = base / (2 * w);
+    const int a = pair * 2 * w;
+    const int la = a < cnt ? (a + w < cnt ? w : cnt - a) : 0;
+    const int b = a + w;
+    const int lb = b < cnt ? (b + w < cnt ? w : cnt - b) : 0;
+    const int d = base - a;
+    const int outs = la + lb - d < MBS_ITEMS ? la + lb - d : MBS_ITEMS;
+    if (outs > 0) {
+      const int i = mbs_split<T>(sk[src] + a, la, sk[src] + b, lb, d);
+      mbs_merge_out<T>(sk[src] + a, si[src] + a, la, sk[src] + b, si[src] + b, lb, i, d - i,
+                       outs, sk[src ^ 1] + base, si[src ^ 1] + base);
+    }
+    __syncthreads();
+    src ^= 1;
+  }
+  for (int q = threadIdx.x; q < cnt; q += MBS_THREADS) {
+    out_k[t0 + q] = sk[src][q];
+    out_i[t0 + q] = si[src][q];
+  }
+}
+// One merge pass: sorted runs of width w -> 2w.
+extern "C" __global__ void mbs_merge_pass(const T* in_k, const unsigned* in_i, T* out_k,
+                                          unsigned* out_i, unsigned long long n,
+                                          unsigned long long w) {
+  __shared__ T sk[2 * MBS_TILE];
+  __shared__ unsigned si[2 * MBS_TILE];
+  __shared__ int s_split[2];
+  const unsigned long long d0 = (unsigned long long)blockIdx.x * MBS_TILE;
+  if (d0 >= n) return;
+  const unsigned long long a = d0 / (2 * w) * (2 * w);
+  const unsigned long long la = a + w < n ? w : n - a;
+  const unsigned long long b = a + la;
+  const unsigned long long lb = b + w < n ? w : (b < n ? n - b : 0);
+  const unsigned long long d1 = d0 + MBS_TILE < a + la + lb ? d0 + MBS_TILE : a + la + lb;
+  if (threadIdx.x < 2) {  // merge-path splits of the tile's two ends, in global memory
+    const unsigned long long d = (threadIdx.x == 0 ? d0 : d1) - a;
+    unsigned long long lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+    while (lo < hi) {
+      const unsigned long long mid = (lo + hi) >> 1;
+      if (!USER_LESS(in_k[b + d - 1 - mid], in_k[a + mid])) lo = mid + 1;
+      else hi = mid;
+    }
+    s_split[threadIdx.x] = (int)lo;
+  }
+  __syncthreads();
+  const unsigned long long i0 = s_split[0], i1 = s_split[1];
+  const unsigned long long j0 = d0 - a - i0, j1 = d1 - a - i1;
+  const int na = (int)(i1 - i0), nb = (int)(j1 - j0);
+  for (int q = threadIdx.x; q < na; q += MBS_THREADS) {
+    sk[q] = in_k[a + i0 + q];
+    si[q] = in_i[a + i0 + q];
+  }
+  for (int q = threadIdx.x; q < nb; q += MBS_THREADS) {
+    sk[na + q] = in_k[b + j0 + q];
+    si[na + q] = in_i[b + j0 + q];
+  }
+  __syncthreads();
+  const int total = na + nb;
+  const int d = threadIdx.x * MBS_ITEMS;
+  if (d < total) {
+    const int outs = total - d < MBS_ITEMS ? total - d : MBS_ITEMS;
+    const int i = mbs_split<T>(sk, na, sk + na, nb, d);
+    T ko[MBS_ITEMS];
+    unsigned io[MBS_ITEMS];
+    mbs_merge_out<T>(sk, si, na, sk + na, si + na, nb, i, d - i, outs, ko, io);
+    for (int q = 0; q < outs; ++q) {
+      out_k[d0 + d + q] = ko[q];
+      out_i[d0 + d + q] = io[q];
+    }
+  }
+}
+)MBJ";
+
 const char* kMapKernels = R"MBJ(
 extern "C" __global__ void mbj_map(const In* in, Out* out, unsigned long long n) {
   for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n;
@@ -268,11 +403,11 @@ int nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::string&
 }  // namespace mb
 
 struct mb_user_op {
-  int kind;       // 0 binary, 1 map
-  int dtype;      // binary: T; map: In
+  int kind;       // 0 binary, 1 map, 2 predicate (a comparator)
+  int dtype;      // binary / predicate: T; map: In
   int out_dtype;  // map: Out
   cudaLibrary_t lib = nullptr;
-  cudaKernel_t k[6] = {};
+  cudaKernel_t k[8] = {};
 };
 
 using namespace mb;
@@ -280,17 +415,22 @@ using namespace mb;
 namespace {
 
 enum { kReducePartial = 0, kReduceFinal = 1, kScanTiles = 2, kScanTotals = 3, kScanApply = 4,
-       kMap = 5 };
+       kMap = 5, kBlockSort = 6, kMergePass = 7 };
+constexpr uint64_t kSortTile = 1024;  // MBS_TILE of kSortKernels
 
 int build_op(int kind, int dtype, int out_dtype, const char* source, const char* name,
              bool load, mb_user_op** out) {
   if (!source || !name) return set_error(MB_ERR_LAUNCH, "missing operator source or name");
   if (!dtype_valid(dtype) || (kind == 1 && !dtype_valid(out_dtype)))
     return set_error(MB_ERR_LAUNCH, "unknown element type");
+  if (kind < 0 || kind > 2) return set_error(MB_ERR_LAUNCH, "unknown operator kind");
   std::string src;
   if (kind == 0) {
     src = std::string("typedef ") + ctype_name(dtype) + " T;\n" + source + "\n#define USER_OP " +
           name + "\n" + kBinaryKernels;
+  } else if (kind == 2) {
+    src = std::string("typedef ") + ctype_name(dtype) + " T;\n" + source +
+          "\n#define USER_LESS " + name + "\n" + kSortKernels;
   } else {
     src = std::string("typedef ") + ctype_name(dtype) + " In;\ntypedef " + ctype_name(out_dtype) +
           " Out;\n" + source + "\n#define USER_MAP " + name + "\n" + kMapKernels;
@@ -310,9 +450,11 @@ int build_op(int kind, int dtype, int out_dtype, const char* source, const char*
     return check_cuda(e, "cudaLibraryLoadData");
   }
   const char* names[] = {"mbj_reduce_partial", "mbj_reduce_final", "mbj_scan_tiles",
-                         "mbj_scan_totals", "mbj_scan_apply", "mbj_map"};
-  for (int i = 0; i < 6; ++i) {
-    if ((kind == 0) != (i < 5)) continue;
+                         "mbj_scan_totals", "mbj_scan_apply", "mbj_map",
+                         "mbs_block_sort", "mbs_merge_pass"};
+  for (int i = 0; i < 8; ++i) {
+    const int owner = i < 5 ? 0 : (i == 5 ? 1 : 2);  // the kind whose source holds kernel i
+    if (owner != kind) continue;
     e = cudaLibraryGetKernel(&op->k[i], op->lib, names[i]);
     if (e != cudaSuccess) {
       cudaLibraryUnload(op->lib);
@@ -399,6 +541,69 @@ int mb_user_map_compile(mb_executor* ex, int in_dtype, int out_dtype, const char
   if (!out) return set_error(MB_ERR_LAUNCH, "missing output handle");
   MB_CUDA(cudaSetDevice(ex->device));
   return build_op(1, in_dtype, out_dtype, source, name, true, out);
+}
+
+int mb_user_pred_compile(mb_executor* ex, int dtype, const char* source, const char* name,
+                         mb_user_op** out) {
+  MB_TRY(check_exec(ex));
+  if (!out) return set_error(MB_ERR_LAUNCH, "missing output handle");
+  MB_CUDA(cudaSetDevice(ex->device));
+  return build_op(2, dtype, dtype, source, name, true, out);
+}
+
+int mb_sort_user(mb_executor* ex, const mb_src* keys, mb_user_op* less, const mb_src* values,
+                 int nvals, mb_col out_keys, const mb_col* out_values) {
+  MB_TRY(check_exec(ex));
+  if (!less || less->kind != 2) return set_error(MB_ERR_LAUNCH, "not a compiled comparator");
+  MB_TRY(check_plain(ex, keys, less->dtype));
+  if (nvals < 0 || nvals > 12) return set_error(MB_ERR_LAUNCH, "values take 0 to 12 columns");
+  const uint64_t n0 = keys->len;
+  for (int c = 0; c < nvals; ++c) {
+    MB_TRY(check_src(ex, &values[c], "values"));
+    MB_TRY(check_col(ex, out_values[c], "value output"));
+    if (values[c].len != n0)
+      return set_error(MB_ERR_LENGTH_MISMATCH, "input lengths differ", n0, values[c].len);
+    if (out_values[c].len < n0)
+      return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", n0,
+                       out_values[c].len);
+  }
+  if (out_keys.data) {
+    MB_TRY(check_col(ex, out_keys, "key output"));
+    if (out_keys.dtype != less->dtype)
+      return set_error(MB_ERR_LAUNCH, "key output element type differs");
+    if (out_keys.len < n0)
+      return set_error(MB_ERR_OUTPUT_TOO_SHORT, "output is shorter than input", n0, out_keys.len);
+  }
+  uint64_t n = n0;
+  if (n == 0) return MB_OK;
+  const size_t es = dtype_size(less->dtype);
+  const size_t kb = (n * es + 255) / 256 * 256, ib = (n * 4 + 255) / 256 * 256;
+  Scratch scratch;
+  MB_TRY(scratch.alloc(ex, 2 * (kb + ib)));
+  char* k0 = scratch.as<char>();
+  char* i0 = k0 + kb;
+  char* k1 = i0 + ib;
+  char* i1 = k1 + kb;
+  const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+  const void* kin = keys->data;
+  void* a0[] = {(void*)&kin, (void*)&n, (void*)&k0, (void*)&i0};
+  MB_TRY(launch(ex, less->k[kBlockSort], (unsigned)tiles, 256, a0));
+  for (uint64_t w = kSortTile; w < n; w <<= 1) {
+    void* a1[] = {(void*)&k0, (void*)&i0, (void*)&k1, (void*)&i1, (void*)&n, (void*)&w};
+    MB_TRY(launch(ex, less->k[kMergePass], (unsigned)tiles, 256, a1));
+    std::swap(k0, k1);
+    std::swap(i0, i1);
+  }
+  if (out_keys.data)
+    MB_CUDA(cudaMemcpyAsync(out_keys.data, k0, n * es, cudaMemcpyDeviceToDevice, ex->stream));
+  mb_src idx{};
+  idx.kind = MB_SRC_COLUMN;
+  idx.dtype = idx.vtype = MB_U32;
+  idx.map = MB_UN_IDENTITY;
+  idx.data = i0;
+  idx.len = n;
+  for (int c = 0; c < nvals; ++c) MB_TRY(mb_gather(ex, &values[c], &idx, nullptr, out_values[c]));
+  return MB_OK;
 }
 
 int mb_user_op_check(int kind, int dtype, int out_dtype, const char* source, const char* name) {

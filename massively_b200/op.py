@@ -116,6 +116,21 @@ class UserOp:
                                           name.encode(), C.byref(h)))
         return cls(h, 1, i, o)
 
+    @classmethod
+    def predicate(cls, exec, dtype, source: str, name: str) -> "UserOp":
+        """A comparator (op::BinaryPredicateOp): `source` defines
+        `__device__ bool name(T a, T b)`, a strict weak order; usable with
+        vector.sort and vector.sort_by_key (stable)."""
+        import ctypes as C
+        import numpy as np
+        from . import _native as N
+        from .runtime import NP_TO_ID, check
+        h = C.c_void_p()
+        dt = np.dtype(dtype)
+        check(N.lib().mb_user_pred_compile(exec.handle, NP_TO_ID[dt], source.encode(),
+                                           name.encode(), C.byref(h)))
+        return cls(h, 2, dt, dt)
+
     @staticmethod
     def check_source(kind: int, dtype, out_dtype, source: str, name: str) -> None:
         """Compiles without loading (no device needed); raises on an error."""

@@ -445,8 +445,16 @@ def radix_sort_pairs(exec: Executor, keys, values):
 
 
 def sort(exec: Executor, input, less=O.Less) -> DeviceVec:
-    """vector::sort (massively/src/api/algorithm/ordering.rs:64): stable."""
+    """vector::sort (massively/src/api/algorithm/ordering.rs:64): stable;
+    `less` a built-in predicate or a compiled comparator
+    (op.UserOp.predicate)."""
     _check_owner(exec, input)
+    if isinstance(less, O.UserOp):
+        x = _plain(exec, input, less.dtype)
+        out = exec.alloc(less.dtype, len(x))
+        check(_L().mb_sort_user(exec.handle, C.byref(x.to_src()), less.handle, None, 0,
+                                out.to_col(), None))
+        return out
     keep = []
     _len(input)
     s = lower(exec, input, keep)
@@ -457,11 +465,20 @@ def sort(exec: Executor, input, less=O.Less) -> DeviceVec:
 
 def sort_by_key(exec: Executor, keys, values, less=O.Less):
     """vector::sort_by_key (by_key.rs:226): the values in the stable order of
-    the keys under `less`."""
+    the keys under `less` (a built-in predicate or a compiled comparator)."""
     _check_owner(exec, keys, values)
     n, m = _len(keys), _len(values)
     if n != m:
         raise LengthMismatch(n, m)
+    if isinstance(less, O.UserOp):
+        x = _plain(exec, keys, less.dtype)
+        keep = []
+        vs, nv = _srcs(exec, values, keep)
+        outs = _out_like(exec, values, n)
+        none = N.mb_col()
+        check(_L().mb_sort_user(exec.handle, C.byref(x.to_src()), less.handle, vs, nv, none,
+                                _cols(outs)))
+        return _wrap(values, outs)
     keep = []
     ks = lower(exec, keys, keep)
     vs, nv = _srcs(exec, values, keep)

@@ -281,3 +281,18 @@ def test_oracle_agrees_with_numpy(orc, n):
     np.testing.assert_array_equal(orc.sort_perm(keys), np.argsort(keys, kind="stable"))
     st = orc.flags(x, "is_even")
     np.testing.assert_array_equal(orc.copy_where(x, st), x[st.astype(bool)])
+
+
+@pytest.mark.parametrize("dtype", [np.uint32, np.int32, np.float32, np.uint64, np.int64,
+                                   np.float64])
+@pytest.mark.parametrize("n,threads", [(0, 4), (1, 3), (1000, 7), (100_003, 8)])
+def test_parallel_stable_order_equals_the_sequential_oracle(orc, dtype, n, threads):
+    """radix_perm_par (the full-size checks' stable order on all host
+    cores) gives the sequential oracle's permutation, ties and signed zeros
+    included."""
+    dt = np.dtype(dtype)
+    if dt.kind == "f":
+        x = (orc.normal_f32(7, n) * 3).round().astype(dt)  # many ties, -0.0 and +0.0
+    else:
+        x = orc.uniform_u32(0, 50, 7, n).astype(dt) - (25 if dt.kind == "i" else 0)
+    np.testing.assert_array_equal(orc.radix_perm_par(x, threads), orc.radix_perm([x]))

@@ -35,3 +35,19 @@ def test_compile_error_is_reported():
         UserOp.check_source(0, np.uint32, np.uint32, "__device__ T broken(T a, T b) { return a +; }",
                             "broken")
     assert "did not compile" in str(e.value)
+
+
+def test_comparator_sources_compile():
+    """A user comparator (kind 2) compiles with the merge-sort kernels; a
+    broken one reports the compiler's message."""
+    from massively_b200.op import UserOp
+    from massively_b200.runtime import Error
+    for dt in (np.uint32, np.float64, np.int16):
+        UserOp.check_source(2, dt, dt, "__device__ bool by_low(T a, T b) { return (a & 7) < (b & 7); }"
+                            if np.dtype(dt).kind in "iu" else
+                            "__device__ bool desc(T a, T b) { return b < a; }",
+                            "by_low" if np.dtype(dt).kind in "iu" else "desc")
+    with pytest.raises(Error) as e:
+        UserOp.check_source(2, np.uint32, np.uint32, "__device__ bool bad(T a, T b) { return a <; }",
+                            "bad")
+    assert "did not compile" in str(e.value)

@@ -99,3 +99,48 @@ def test_user_op_errors(ex):
         check(N.lib().mb_inclusive_scan_user(ex.handle, C.byref(d.to_src()), m.handle,
                                              out.to_col()))
     assert int(vector.reduce(ex, d, np.uint32(0), sat)) == 45
+
+
+# ------------------------------------------------------- user comparators --
+
+BY_MOD = "__device__ bool by_mod(T a, T b) { return (a % 1000u) < (b % 1000u); }"
+DESC = "__device__ bool desc(T a, T b) { return b < a; }"
+BY_HIGH = "__device__ bool by_high(T a, T b) { return (a >> 32) < (b >> 32); }"
+
+
+@pytest.mark.parametrize("n", [1, 2, 1023, 1024, 1025, 4097, 100_003, 1 << 20])
+def test_user_comparator_sort_is_stable(ex, n):
+    """vector::sort / sort_by_key under a user comparator with many ties
+    (keys compared mod 1000): the stable order, values carried."""
+    from massively_b200 import lazy, op, vector, zip2
+    less = op.UserOp.predicate(ex, np.uint32, BY_MOD, "by_mod")
+    keys = seeded(np.uint32, n, 40)
+    want = np.argsort(keys % 1000, kind="stable")
+    dk = ex.to_device(keys)
+    np.testing.assert_array_equal(ex.to_host(vector.sort(ex, dk, less)), keys[want])
+    vals = zip2(ex.to_device(np.arange(n, dtype=np.uint32)), lazy.counting(7).take(n))
+    a, b = vector.sort_by_key(ex, dk, vals, less).into_columns()
+    np.testing.assert_array_equal(ex.to_host(a), want.astype(np.uint32))
+    np.testing.assert_array_equal(ex.to_host(b), (want + 7).astype(np.uint32))
+
+
+@pytest.mark.parametrize("dtype,src,name,pred", [(np.float64, DESC, "desc", "greater"),
+                                                 (np.int32, DESC, "desc", "greater")])
+def test_user_comparator_matches_builtin_order(ex, orc, dtype, src, name, pred):
+    from massively_b200 import op, vector
+    less = op.UserOp.predicate(ex, dtype, src, name)
+    x = seeded(dtype, 300_007, 41)
+    got = ex.to_host(vector.sort_by_key(ex, ex.to_device(x),
+                                        ex.to_device(np.arange(x.size, dtype=np.uint32)), less))
+    np.testing.assert_array_equal(got, orc.sort_perm(x, pred))
+
+
+def test_user_comparator_on_packed_u64(ex):
+    """Only the high halves order the items; the low halves show the
+    input order of ties."""
+    from massively_b200 import op, vector
+    less = op.UserOp.predicate(ex, np.uint64, BY_HIGH, "by_high")
+    hi = seeded(np.uint32, 50_000, 42) % np.uint32(50)
+    x = (hi.astype(np.uint64) << np.uint64(32)) | np.arange(hi.size, dtype=np.uint64)
+    got = ex.to_host(vector.sort(ex, ex.to_device(x), less))
+    np.testing.assert_array_equal(got, x[np.argsort(hi, kind="stable")])
