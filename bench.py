@@ -432,6 +432,8 @@ class SegScanF32(Workload):
         self.metric = "segmented GB/s"
         self.unit = "GB/s"
         self.dtype = "u32" if mode == "sort" else "f32"
+        if mode == "sort":
+            self.kernel = "ss_kernel"
 
     def setup(self, ex):
         from massively_b200 import seg

@@ -616,7 +616,8 @@ enum {
   MB_KF_RADIX_HISTOGRAM = 1, /* the all-digit histogram */
   MB_KF_SCAN = 2,            /* inclusive / exclusive scan */
   MB_KF_SELECT = 3,          /* copy_where / remove_where / partition */
-  MB_KF_SEARCH = 4           /* first-index searches and extrema (predicate.cu) */
+  MB_KF_SEARCH = 4,          /* first-index searches and extrema (predicate.cu) */
+  MB_KF_SEG_SORT = 5         /* the segmented sort of 4-byte values (segsort.cu) */
 };
 int mb_kernel_timing(mb_executor* exec, int enable);
 int mb_kernel_timing_read(mb_executor* exec, int family, uint64_t* launches, double* total_ms);

@@ -51,13 +51,20 @@ constexpr int kSegMinBlocks = 4;
 // its tail fold; seg_tile_carry_kernel scans those folds over the tiles
 // (a segmented scan of one value per tile), and seg_scan_fix_kernel applies
 // each tile's carry to the items before its first segment start.
+// kReduceKeysTiles: reduce_by_key the same way -- a first pass counts every
+// tile's run heads (seg_run_heads_kernel) and scans the counts into each
+// tile's first run index (seg_run_base_kernel); each tile then reduces the
+// runs that start and end in it and leaves its folds for the runs that cross
+// its edges (seg_rbk_walk_kernel).  The run bases are computed once per call
+// and shared by every value column of the same tile size.
 enum SegMode : int {
   kScanIncl = 0,
   kScanExcl = 1,
   kReduce = 2,
   kReduceTiles = 3,
   kScanInclTiles = 4,
-  kScanExclTiles = 5
+  kScanExclTiles = 5,
+  kReduceKeysTiles = 6
 };
 enum HeadsSrc : int { kHeadsOffsets = 0, kHeadsKeys = 1 };
 
@@ -130,6 +137,10 @@ struct SegParams {
   V* part_head;
   V* part_tail;
   uint32_t* tail_seg;
+  // kReduceKeysTiles: each tile's first run index (the heads before it) and
+  // the position of its first head (the tile's length when it has none).
+  const uint32_t* run_base;
+  uint32_t* first_pos;
 };
 
 __device__ __forceinline__ bool key_eq(int dtype, uint64_t a, uint64_t b) {
@@ -360,7 +371,8 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
   }
 
   const Op<V, OP> vop{p.op};
-  if (p.mode == kScanIncl || p.mode == kScanExcl || p.mode >= kScanInclTiles) {
+  if (p.mode == kScanIncl || p.mode == kScanExcl || p.mode == kScanInclTiles ||
+      p.mode == kScanExclTiles) {
     V o[kLoads][VEC];
     if (p.mode == kScanIncl || p.mode == kScanInclTiles) {
 #pragma unroll
@@ -459,6 +471,36 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
         p.part_tail[tile] = stage[te - tb - 1].v;
       }
     }
+  } else if (local) {
+    // kReduceKeysTiles: run index = the tile's first run index + the tile-
+    // local inclusive head count - 1.  Items before the tile's first head
+    // belong to the run that came in from an earlier tile.
+    const uint32_t base = p.run_base[tile];
+    for (uint64_t i = tb + tid; i < te; i += kThreads) {
+      const uint32_t pos = (uint32_t)(i - tb);
+      const T yv = stage[pos];
+      const bool head = (s_bits[pos >> 5] >> (pos & 31)) & 1u;
+      if (head && p.out_keys)
+        st_raw_bits(p.out_keys, base + yv.heads - 1, p.out_key_esize, src_load_bits(p.keys, i));
+      const bool last = i + 1 == te;
+      const bool tail = last ? (s_head_te != 0)
+                             : (((s_bits[(pos + 1) >> 5] >> ((pos + 1) & 31)) & 1u) != 0);
+      if (yv.heads == 0) {
+        if (tail || last) p.part_head[tile] = yv.v;  // the incoming run's part here
+      } else if (tail) {
+        st_cast<V>(p.out_dtype, p.out, base + yv.heads - 1, vop(p.init, yv.v));
+      } else if (last) {
+        p.tail_seg[tile] = base + yv.heads - 1;  // goes on past this tile
+      }
+      if (last) p.part_tail[tile] = yv.v;
+    }
+    __shared__ uint32_t s_fp;  // the tile's first head
+    if (tid == 0) s_fp = (uint32_t)(te - tb);
+    __syncthreads();
+    if (tid < C::TILE / 32 && s_bits[tid])
+      atomicMin(&s_fp, (uint32_t)tid * 32 + __ffs(s_bits[tid]) - 1);
+    __syncthreads();
+    if (tid == 0) p.first_pos[tile] = s_fp;
   } else {
     // Runs of equal keys: key at the head, value at the tail, index =
     // inclusive head count - 1.
@@ -480,7 +522,9 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
 
 template <class V>
 size_t seg_smem(int mode) {
-  return mode == kReduce || mode == kReduceTiles ? sizeof(SegVal<V>) * SegCfg<V>::TILE : 0;
+  return mode == kReduce || mode == kReduceTiles || mode == kReduceKeysTiles
+             ? sizeof(SegVal<V>) * SegCfg<V>::TILE
+             : 0;
 }
 
 // kReduceTiles: the segments that cross tile edges, one thread per tile
@@ -506,6 +550,161 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// One block scans per-tile values over all tiles (carries, run bases).
+constexpr int kCarryThreads = 1024;
+
+// kReduceKeysTiles, first pass: the run heads of every tile -- items whose
+// key differs from the one before (massively's Equal; the first item is a
+// head) and, for reduce_by_key_segmented, segment starts -- counted into
+// head_count[tile].
+__global__ void __launch_bounds__(kThreads)
+    seg_run_heads_kernel(Src keys, uint64_t cap, const uint32_t* __restrict__ n_dev,
+                         const uint32_t* __restrict__ offsets, uint64_t nseg,
+                         const uint32_t* __restrict__ tile_lb, uint64_t tile_items,
+                         uint32_t* __restrict__ head_count) {
+  constexpr int kMaxWords = 4096 / 32;  // the largest tile (4-byte values)
+  __shared__ uint32_t s_bits[kMaxWords];
+  __shared__ uint32_t s_cnt;
+  const uint64_t tile = blockIdx.x;
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t tb = tile * tile_items;
+  if (tb >= n) return;
+  const uint64_t te = min(tb + tile_items, n);
+  const int words = (int)(tile_items / 32);
+  for (int w = threadIdx.x; w < words; w += kThreads) s_bits[w] = 0;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  for (uint64_t i = tb + threadIdx.x; i < te; i += kThreads) {
+    bool h = i == 0;
+    if (!h) h = !key_eq(keys.vtype, src_load_bits(keys, i - 1), src_load_bits(keys, i));
+    if (h) atomicOr(&s_bits[(i - tb) >> 5], 1u << ((i - tb) & 31));
+  }
+  if (offsets) {
+    const uint64_t sa = tile_lb[tile];
+    const uint64_t sb = te == n ? nseg : min((uint64_t)tile_lb[tile + 1], nseg);
+    for (uint64_t s = sa + threadIdx.x; s < sb; s += kThreads) {
+      const uint64_t start = offsets[s];
+      if (start >= tb && start < te) atomicOr(&s_bits[(start - tb) >> 5], 1u << ((start - tb) & 31));
+    }
+  }
+  __syncthreads();
+  uint32_t c = 0;
+  for (int w = threadIdx.x; w < words; w += kThreads) c += __popc(s_bits[w]);
+  c = __reduce_add_sync(kFull, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_cnt, c);
+  __syncthreads();
+  if (threadIdx.x == 0) head_count[tile] = s_cnt;
+}
+
+// kReduceKeysTiles: head counts -> each tile's first run index (exclusive
+// sum, in place over `counts`) and the run count to counts[live] and
+// count_dev.  One block:
+// each thread sums a contiguous run of tiles, a block scan joins them.
+__global__ void __launch_bounds__(kCarryThreads)
+    seg_run_base_kernel(uint32_t* __restrict__ counts, uint64_t tiles, uint64_t tile_items,
+                        uint64_t cap, const uint32_t* __restrict__ n_dev,
+                        uint32_t* __restrict__ count_dev) {
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t live = min((n + tile_items - 1) / tile_items, tiles);
+  const uint64_t per = (live + blockDim.x - 1) / blockDim.x;
+  const uint64_t u0 = threadIdx.x * per, u1 = min(u0 + per, live);
+  uint32_t sum = 0;
+  for (uint64_t u = u0; u < u1; ++u) sum += counts[u];
+  __shared__ uint32_t s_v[kCarryThreads];
+  s_v[threadIdx.x] = sum;
+  __syncthreads();
+  for (int d = 1; d < (int)blockDim.x; d <<= 1) {
+    const uint32_t x = threadIdx.x >= (unsigned)d ? s_v[threadIdx.x - d] : 0u;
+    __syncthreads();
+    s_v[threadIdx.x] += x;
+    __syncthreads();
+  }
+  uint32_t run = s_v[threadIdx.x] - sum;  // exclusive
+  for (uint64_t u = u0; u < u1; ++u) {
+    const uint32_t c = counts[u];
+    counts[u] = run;
+    run += c;
+  }
+  if (threadIdx.x == blockDim.x - 1) {
+    counts[live] = s_v[threadIdx.x];  // the run count, after the last tile's base
+    if (count_dev) *count_dev = s_v[threadIdx.x];
+  }
+}
+
+// kReduceKeysTiles: the runs that cross tile edges.  One block scans
+// (has a head, tail fold) over the tiles -- the segmented scan of
+// seg_tile_carry_kernel -- so `run` is the fold of the run still open at the
+// end of tile u - 1.  That run ends in the first later tile with a head
+// (after the fold of the items before that head, part_head) or at the end of
+// the data; it is written there unless it ended exactly at the end of a tile
+// that wrote it itself (a head in tile u - 1 and one at the start of tile
+// u).  Work is O(tiles) whatever the run lengths.
+template <class V>
+__global__ void __launch_bounds__(kCarryThreads)
+    seg_rbk_walk_kernel(uint64_t tiles, uint64_t tile_items, uint64_t cap,
+                        const uint32_t* __restrict__ n_dev, int op, V init,
+                        const V* __restrict__ part_head, const V* __restrict__ part_tail,
+                        const uint32_t* __restrict__ first_pos,
+                        const uint32_t* __restrict__ run_base, void* out, int out_dtype) {
+  using T = SegVal<V>;
+  const SegOp<V, kOpDyn> sop{Op<V, kOpDyn>{op}};
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t live = min((n + tile_items - 1) / tile_items, tiles);
+  if (live == 0) return;
+  const uint64_t per = (live + kCarryThreads - 1) / kCarryThreads;
+  const uint64_t u0 = threadIdx.x * per, u1 = min(u0 + per, live);
+  auto has_head = [&](uint64_t u) -> bool {
+    return (uint64_t)first_pos[u] < min(tile_items, n - u * tile_items);
+  };
+  T agg{0, V(0)};
+  bool has = false;
+  for (uint64_t u = u0; u < u1; ++u) {
+    const T x{has_head(u) ? 1u : 0u, part_tail[u]};
+    agg = has ? sop(agg, x) : x;
+    has = true;
+  }
+  __shared__ T s_v[kCarryThreads];
+  __shared__ int s_h[kCarryThreads];
+  s_v[threadIdx.x] = agg;
+  s_h[threadIdx.x] = has;
+  __syncthreads();
+  for (int d = 1; d < kCarryThreads; d <<= 1) {  // inclusive, in thread order
+    T x{};
+    int hx = 0;
+    if (threadIdx.x >= d && s_h[threadIdx.x - d]) {
+      x = s_h[threadIdx.x] ? sop(s_v[threadIdx.x - d], s_v[threadIdx.x]) : s_v[threadIdx.x - d];
+      hx = 1;
+    }
+    __syncthreads();
+    if (hx) {
+      s_v[threadIdx.x] = x;
+      s_h[threadIdx.x] = 1;
+    }
+    __syncthreads();
+  }
+  T run{0, V(0)};
+  bool rh = threadIdx.x > 0 && s_h[threadIdx.x - 1];
+  if (rh) run = s_v[threadIdx.x - 1];
+  bool prev_head = u0 > 0 && u0 < u1 && has_head(u0 - 1);
+  for (uint64_t u = u0; u < u1; ++u) {
+    const bool hh = has_head(u);
+    if (u > 0 && hh) {
+      const uint32_t fp = first_pos[u];
+      if (fp > 0 || !prev_head)
+        st_cast<V>(out_dtype, out, run_base[u] - 1,
+                   op_apply_rt<V>(op, init, fp > 0 ? op_apply_rt<V>(op, run.v, part_head[u])
+                                                   : run.v));
+    }
+    const T x{hh ? 1u : 0u, part_tail[u]};
+    run = rh ? sop(run, x) : x;
+    rh = true;
+    prev_head = hh;
+  }
+  // The last run, when no head in the last tile let that tile write it.
+  if (u0 < u1 && u1 == live && !prev_head)
+    st_cast<V>(out_dtype, out, run_base[live] - 1, op_apply_rt<V>(op, init, run.v));
+}
+
 // Whether tile t (items [t * tile_items, te)) holds a segment start: the
 // first start at or after its beginning lies before its end.
 __device__ __forceinline__ bool tile_has_start(const uint32_t* offsets, const uint32_t* tile_lb,
@@ -513,7 +712,6 @@ __device__ __forceinline__ bool tile_has_start(const uint32_t* offsets, const ui
   return (uint64_t)offsets[tile_lb[t]] < te;
 }
 
-constexpr int kCarryThreads = 1024;
 
 // kScan*Tiles: carry[t] = the fold of the segment that enters tile t over
 // the items before t -- the value of an inclusive segmented scan, over the
@@ -625,8 +823,17 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// kReduceKeysTiles: run bases shared by the value columns of one
+// reduce_by_key call (`ptr` holds tiles + 1 words for the smallest tile;
+// `tile` is the tile size they were computed for, 0 before the first).
+struct RunBases {
+  uint32_t* ptr = nullptr;
+  uint64_t tile = 0;
+};
+
 template <class V>
-int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_wide) {
+int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_wide,
+            RunBases* rb) {
   using C = SegCfg<V>;
   const uint64_t cap = in.len;
   if (cap == 0) return MB_OK;
@@ -640,12 +847,15 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   const size_t lb_b = p.offsets ? ((tiles + 1) * 4 + 255) / 256 * 256 : 0;
   // kReduceTiles: part_head, part_tail, tail_seg; kScan*Tiles: part_tail and
   // the carries (in the part_head slot).
-  const bool scan_tiles = p.mode >= kScanInclTiles;
-  const bool tiles_mode = p.mode == kReduceTiles || scan_tiles;
+  const bool scan_tiles = p.mode == kScanInclTiles || p.mode == kScanExclTiles;
+  const bool keys_tiles = p.mode == kReduceKeysTiles;
+  const bool tiles_mode = p.mode == kReduceTiles || scan_tiles || keys_tiles;
   const size_t part_b = tiles_mode ? (tiles * sizeof(V) + 255) / 256 * 256 : 0;
   const size_t tseg_b = tiles_mode ? (tiles * 4 + 255) / 256 * 256 : 0;
+  // kReduceKeysTiles: run bases (tiles + 1 words) and first-head positions
+  const size_t keys_b = keys_tiles ? 2 * (((tiles + 1) * 4 + 255) / 256 * 256) : 0;
   Scratch scratch;
-  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b + 2 * part_b + tseg_b));
+  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b + 2 * part_b + tseg_b + keys_b));
   MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + state_b, ex->stream));
   p.counter = scratch.as<uint32_t>();
   p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
@@ -655,6 +865,14 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
     p.part_tail = (V*)(q + part_b);
     p.tail_seg = (uint32_t*)(q + 2 * part_b);
     MB_CUDA(cudaMemsetAsync(p.tail_seg, 0xFF, tiles * 4, ex->stream));
+    if (keys_tiles) {
+      uint32_t* base = (uint32_t*)(q + 2 * part_b + tseg_b);
+      p.first_pos = (uint32_t*)((char*)base + keys_b / 2);
+      if (rb && rb->ptr) base = rb->ptr;
+      p.run_base = base;
+      if (!rb || rb->tile != (uint64_t)C::TILE)
+        MB_CUDA(cudaMemsetAsync(base, 0, (tiles + 1) * 4, ex->stream));
+    }
   }
   if (p.offsets) {
     uint32_t* lb = (uint32_t*)(scratch.as<char>() + 256 + state_b);
@@ -666,9 +884,19 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
     p.tile_lb = lb;
   }
   const bool plain = src_plain(in, DTypeOf<V>::value) && (uintptr_t)in.data % 16 == 0 &&
-                     (p.mode == kReduce || p.mode == kReduceTiles ||
+                     (p.mode == kReduce || p.mode == kReduceTiles || keys_tiles ||
                       (uintptr_t)p.out % 16 == 0);
   const Src s = to_src(in);
+  if (keys_tiles && (!rb || rb->tile != (uint64_t)C::TILE)) {
+    // Every tile's first run index, and the run count.
+    if (rb && rb->ptr) rb->tile = C::TILE;
+    seg_run_heads_kernel<<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
+        p.keys, cap, in.len_dev, p.offsets, p.nseg, p.tile_lb, C::TILE, (uint32_t*)p.run_base);
+    MB_CUDA(cudaGetLastError());
+    seg_run_base_kernel<<<1, kCarryThreads, 0, ex->stream>>>(
+        (uint32_t*)p.run_base, tiles, C::TILE, cap, in.len_dev, p.count_dev);
+    MB_CUDA(cudaGetLastError());
+  }
   const size_t smem = seg_smem<V>(p.mode);
   char* state_base = scratch.as<char>() + 256;
   auto launch = [&](auto kern, auto st) -> int {
@@ -709,6 +937,11 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
           p.mode == kScanExclTiles ? 1 : 0, p.init, p.part_head, p.out, p.out_dtype);
       MB_CUDA(cudaGetLastError());
     }
+  } else if (keys_tiles) {
+    seg_rbk_walk_kernel<V><<<1, kCarryThreads, 0, ex->stream>>>(
+        tiles, C::TILE, cap, in.len_dev, p.op, p.init, p.part_head, p.part_tail, p.first_pos,
+        p.run_base, p.out, p.out_dtype);
+    MB_CUDA(cudaGetLastError());
   } else if (tiles_mode) {
     const unsigned g = (unsigned)std::min<uint64_t>((tiles + kThreads - 1) / kThreads, 4096);
     seg_reduce_cross_kernel<V><<<std::max(1u, g), kThreads, 0, ex->stream>>>(
@@ -723,7 +956,8 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
 // (scans) or per-segment / per-run results (reductions).
 int seg_entry(mb_executor* ex, const mb_src* values, int op, int mode, const void* init,
               void* out, int out_dtype, const uint32_t* offsets, uint64_t nseg,
-              const mb_src* keys, void* out_keys, int out_key_esize, uint32_t* count_dev) {
+              const mb_src* keys, void* out_keys, int out_key_esize, uint32_t* count_dev,
+              RunBases* rb = nullptr) {
   const int ct = compute_type(values->vtype);
   if (!op_valid_for(op, ct)) return set_error(MB_ERR_LAUNCH, "operator not defined for this type");
   uint64_t init_wide = 0;
@@ -750,7 +984,7 @@ int seg_entry(mb_executor* ex, const mb_src* values, int op, int mode, const voi
     p.out_keys = out_keys;                                          \
     p.out_key_esize = out_key_esize;                                \
     p.count_dev = count_dev;                                        \
-    return seg_run<V>(ex, *values, p, &init_wide);                  \
+    return seg_run<V>(ex, *values, p, &init_wide, rb);              \
   }
   switch (ct) {
     case MB_U32: MB_SEG_DISPATCH(uint32_t)
@@ -1159,15 +1393,30 @@ int mb_reduce_by_key_segmented(mb_executor* ex, const mb_src* keys, int key_eq,
   if (n == 0) {
     MB_CUDA(cudaMemsetAsync(count_dev, 0, 4, ex->stream));
   } else {
+    // MB_TUNE_SEG: 0 = tile-local runs plus the crossing-run pass (default),
+    // 1 = the segmented scan's look-back carried across tiles
+    const int mode = ex->tune[MB_TUNE_SEG] == 1 ? kReduce : kReduceKeysTiles;
+    Scratch bases;
+    RunBases rb;
+    // Shared when every column ends where the keys do (the heads pass reads
+    // the column's device length).
+    bool same_len = true;
+    for (int c = 0; c < nvals; ++c)
+      same_len = same_len && (!values[c].len_dev || values[c].len_dev == keys->len_dev);
+    if (mode == kReduceKeysTiles && nvals > 1 && same_len) {
+      const uint64_t min_tile = SegCfg<uint64_t>::TILE;  // 8-byte values: the smallest
+      MB_TRY(bases.alloc(ex, ((n + min_tile - 1) / min_tile + 1) * 4));
+      rb.ptr = bases.as<uint32_t>();
+    }
     for (int c = 0; c < nvals; ++c) {
       // The keys' device length (a count left by an earlier step) bounds
       // value views that carry none, such as a constant column.
       mb_src v = values[c];
       if (!v.len_dev) v.len_dev = keys->len_dev;
-      MB_TRY(seg_entry(ex, &v, ops[c], kReduce, &inits[c], out_values[c].data,
+      MB_TRY(seg_entry(ex, &v, ops[c], mode, &inits[c], out_values[c].data,
                        out_values[c].dtype, offsets, segment_count, keys,
                        c == 0 ? out_keys.data : nullptr,
-                       (int)dtype_size(out_keys.dtype), c == 0 ? count_dev : nullptr));
+                       (int)dtype_size(out_keys.dtype), c == 0 ? count_dev : nullptr, &rb));
     }
   }
   if (count_host) MB_TRY(read_u32(ex, count_dev, count_host));

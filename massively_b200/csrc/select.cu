@@ -63,6 +63,8 @@ __device__ __forceinline__ void st_raw(void* p, uint64_t i, int esize, uint64_t 
 // NC > 0: NC plain 4-byte columns (all of them), flags fused on column 0 or
 // a plain u32 stencil; every column's items are loaded before the look-back,
 // so their latency overlaps it.  NC = 0: any columns and views, loaded after.
+// Only NC = 1 (an unaligned column) and NC = 0 are launched: two or more
+// preloaded columns cost more registers than the staged kernel below.
 template <int NC>
 __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t cap,
                                                           TileState<uint32_t, true> st) {
@@ -162,8 +164,8 @@ __global__ void __launch_bounds__(kThreads) select_kernel(SelParams p, uint64_t 
 }
 
 // Fast path for plain 16-byte-aligned columns: one CTA per 32 KB tile of
-// one 4-byte column (plus its u32 stencil unless the predicate is fused on
-// the column).  Thread 0 fetches the tile(s) into shared memory with
+// one or two 4-byte columns (plus their u32 stencil unless the predicate is
+// fused on column 0).  Thread 0 fetches the tile(s) into shared memory with
 // cp.async.bulk, so bytes in flight cost no registers; the CTA counts its
 // kept rows from shared memory, runs the look-back, then re-evaluates the
 // flags from shared memory and writes the kept rows.
@@ -187,16 +189,19 @@ __device__ __forceinline__ void sel_named_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-template <bool FUSED, int PRED>
+// NCOL (1 or 2) 4-byte data columns; the stencil tile follows them in
+// shared memory unless the predicate is fused on column 0.
+template <bool FUSED, int PRED, int NCOL>
 __global__ void __launch_bounds__(kThreads + 32)
-    select_smem_kernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ stencil,
-                       uint32_t* __restrict__ out, uint64_t n, int fused_map, int in_dtype,
+    select_smem_kernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ in1,
+                       const uint32_t* __restrict__ stencil, uint32_t* __restrict__ out,
+                       uint32_t* __restrict__ out1, uint64_t n, int fused_map, int in_dtype,
                        uint32_t invert, uint32_t* count_dev, uint32_t* counter, DevErr err,
                        TileState<uint32_t, true> st) {
-  constexpr int kCols = FUSED ? 1 : 2;
+  constexpr int kCols = NCOL + (FUSED ? 0 : 1);
   constexpr int kTileBytes = kSmemTile * 4;
   extern __shared__ __align__(128) unsigned char sel_smem[];
-  uint32_t* buf = reinterpret_cast<uint32_t*>(sel_smem);  // [col][kSmemTile]
+  uint32_t* buf = reinterpret_cast<uint32_t*>(sel_smem);  // [col][kSmemTile], stencil last
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_wcount[kWarps];
@@ -211,8 +216,10 @@ __global__ void __launch_bounds__(kThreads + 32)
     if ((uint64_t)(t + 1) * kSmemTile <= n) {
       mbar_arrive_expect_tx(&bar, kCols * kTileBytes);
       bulk_load(buf, in + (uint64_t)t * kSmemTile, kTileBytes, &bar);
+      if constexpr (NCOL == 2)
+        bulk_load(buf + kSmemTile, in1 + (uint64_t)t * kSmemTile, kTileBytes, &bar);
       if constexpr (!FUSED)
-        bulk_load(buf + kSmemTile, stencil + (uint64_t)t * kSmemTile, kTileBytes, &bar);
+        bulk_load(buf + NCOL * kSmemTile, stencil + (uint64_t)t * kSmemTile, kTileBytes, &bar);
     }
   }
   __syncthreads();
@@ -237,12 +244,13 @@ __global__ void __launch_bounds__(kThreads + 32)
       for (int i = threadIdx.x; i < kSmemTile; i += kThreads) {
         const bool ok = tile_base + i < n;
         buf[i] = ok ? in[tile_base + i] : 0u;
-        if constexpr (!FUSED) buf[kSmemTile + i] = ok ? stencil[tile_base + i] : 0u;
+        if constexpr (NCOL == 2) buf[kSmemTile + i] = ok ? in1[tile_base + i] : 0u;
+        if constexpr (!FUSED) buf[NCOL * kSmemTile + i] = ok ? stencil[tile_base + i] : 0u;
       }
       sel_named_sync(1, kThreads);
     }
     const uint32_t* wv = buf + warp * 32 * kSmemItems;
-    const uint32_t* ws = wv + kSmemTile;
+    const uint32_t* ws = wv + NCOL * kSmemTile;
     auto flag = [&](int k) -> bool {
       if (!full) {
         const uint64_t i = tile_base + (uint64_t)warp * 32 * kSmemItems + k * 32 + lane;
@@ -286,7 +294,11 @@ __global__ void __launch_bounds__(kThreads + 32)
 #pragma unroll 8
   for (int k = 0; k < kSmemItems; ++k) {
     const unsigned b = __shfl_sync(kFull, my_ballot, k);
-    if ((b >> lane) & 1u) out[run + __popc(b & lt)] = wv[k * 32 + lane];
+    if ((b >> lane) & 1u) {
+      const uint32_t o = run + __popc(b & lt);
+      out[o] = wv[k * 32 + lane];
+      if constexpr (NCOL == 2) out1[o] = wv[kSmemTile + k * 32 + lane];
+    }
     run += __popc(b);
   }
 }
@@ -337,7 +349,7 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
     p.fused_map = stencil->map;
     // Every column plain, 4 bytes wide, without a device length; the flags
     // fused on column 0 or a plain u32 stencil.
-    bool plain4 = ncols <= 3 &&
+    bool plain4 = ncols <= 2 &&
                   (p.fused || (src_plain(*stencil, MB_U32) && stencil->vtype == MB_U32 &&
                                stencil->dtype == MB_U32 && stencil->len_dev == nullptr));
     for (int c = 0; c < ncols && plain4; ++c)
@@ -351,38 +363,42 @@ int select_entry(mb_executor* ex, const mb_src* in, int ncols, const mb_src* ste
     p.counter = scratch.as<uint32_t>();
     p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
     auto st = TileState<uint32_t, true>::make(scratch.as<char>() + 256, tiles);
-    const bool aligned = (uintptr_t)in[0].data % 16 == 0 &&
-                         (p.fused || (uintptr_t)stencil->data % 16 == 0);
+    bool aligned = p.fused || (uintptr_t)stencil->data % 16 == 0;
+    for (int c = 0; c < ncols; ++c) aligned = aligned && (uintptr_t)in[c].data % 16 == 0;
     TimedLaunch timed(ex, MB_KF_SELECT);
-    if (fast && aligned && mode != kPartition) {
-      const int cols = p.fused ? 1 : 2;
+    if (plain4 && aligned && mode != kPartition) {
+      // Tiles staged by TMA bulk copies: one per column and one for the stencil.
+      static_assert(kSmemTile >= kTile, "the tile-state array is sized for kTile tiles");
+      const int cols = ncols + (p.fused ? 0 : 1);
       const size_t smem = (size_t)cols * kSmemTile * 4;
       const uint64_t stiles = (n + kSmemTile - 1) / kSmemTile;
+      const uint32_t* in1 = ncols == 2 ? (const uint32_t*)in[1].data : nullptr;
+      uint32_t* out1 = ncols == 2 ? (uint32_t*)out[1].data : nullptr;
       auto launch = [&](auto kern) -> int {
         MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<(unsigned)stiles, kThreads + 32, smem, ex->stream>>>(
-            (const uint32_t*)in[0].data, (const uint32_t*)stencil->data, (uint32_t*)out[0].data, n,
-            stencil->map, in[0].dtype, mode == kRemove ? 1u : 0u, count_dev, p.counter, p.err, st);
+            (const uint32_t*)in[0].data, in1, (const uint32_t*)stencil->data,
+            (uint32_t*)out[0].data, out1, n, stencil->map, in[0].dtype,
+            mode == kRemove ? 1u : 0u, count_dev, p.counter, p.err, st);
         MB_CUDA(cudaGetLastError());
         return MB_OK;
       };
       const bool int4 = in[0].dtype == MB_U32 || in[0].dtype == MB_I32;
-      if (!p.fused) MB_TRY(launch(select_smem_kernel<false, -1>));
+      if (ncols == 2) {
+        if (!p.fused) MB_TRY(launch(select_smem_kernel<false, -1, 2>));
+        else MB_TRY(launch(select_smem_kernel<true, -1, 2>));
+      } else if (!p.fused) MB_TRY(launch(select_smem_kernel<false, -1, 1>));
       else if (int4 && stencil->map == MB_UN_IS_EVEN)
-        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_EVEN>));
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_EVEN, 1>));
       else if (int4 && stencil->map == MB_UN_IS_ODD)
-        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_ODD>));
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_ODD, 1>));
       else if (int4 && stencil->map == MB_UN_IS_TRUE)
-        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_TRUE>));
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_TRUE, 1>));
       else if (int4 && stencil->map == MB_UN_IS_FALSE)
-        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_FALSE>));
-      else MB_TRY(launch(select_smem_kernel<true, -1>));
+        MB_TRY(launch(select_smem_kernel<true, MB_UN_IS_FALSE, 1>));
+      else MB_TRY(launch(select_smem_kernel<true, -1, 1>));
     } else if (fast) {
       select_kernel<1><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
-    } else if (plain4 && ncols == 2) {
-      select_kernel<2><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
-    } else if (plain4 && ncols == 3) {
-      select_kernel<3><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
     } else {
       select_kernel<0><<<(unsigned)tiles, kThreads, 0, ex->stream>>>(p, n, st);
     }

@@ -40,6 +40,8 @@ int seg_ids_fill(mb_executor* ex, const uint32_t* offsets, uint64_t nseg, uint64
                  uint64_t* comp);
 int seg_decode_u32(mb_executor* ex, const uint64_t* comp, uint64_t n, int enc, int desc,
                    uint32_t* out);
+int seg_sort_sized(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
+                   uint64_t nseg, int enc, int desc, int ieee, uint32_t* out, bool* done);
 
 namespace {
 
@@ -257,11 +259,13 @@ int mb_sort(mb_executor* ex, const mb_src* keys, int less, mb_col out) {
   return sort_general(ex, keys, 1, &ieee, &desc, nullptr, 0, nullptr, &out);
 }
 
-// ForEachSegment(Sort(less)) (massively/src/seg/mod.rs:379-425): a stable
-// order of (segment id, value) pairs -- the segment id primary -- sorts every
-// segment in place of massively's two global comparison sorts and three
-// permutation applications.  Segment ids need ceil(log2(segments)/8) digit
-// passes; constant high digits are skipped by the onesweep plan.
+// ForEachSegment(Sort(less)) (massively/src/seg/mod.rs:379-425).  4-byte
+// values are sorted where they lie, in shared memory (segsort.cu).  Other
+// types, and 4-byte calls with a segment too long for one CTA, take a stable
+// global radix sort of (segment id, value) pairs -- the segment id primary --
+// in place of massively's two global comparison sorts and three permutation
+// applications.  Segment ids need ceil(log2(segments)/8) digit passes;
+// constant high digits are skipped by the onesweep plan.
 int mb_seg_sort(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
                 uint64_t segment_count, int less, mb_col out) {
   MB_TRY(check_exec(ex));
@@ -283,6 +287,10 @@ int mb_seg_sort(mb_executor* ex, const mb_src* values, const uint32_t* offsets,
     int ieee = 0, desc = 0;
     comparator_mode(less, vt, &ieee, &desc);
     const int enc = vt == MB_U32 ? 0 : vt == MB_I32 ? 1 : 2;
+    bool done = false;
+    MB_TRY(seg_sort_sized(ex, values, offsets, segment_count, enc, desc, ieee,
+                          (uint32_t*)out.data, &done));
+    if (done) return MB_OK;
     Scratch comp, sorted;
     MB_TRY(comp.alloc(ex, n * 8));
     MB_TRY(sorted.alloc(ex, n * 8));
