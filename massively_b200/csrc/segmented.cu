@@ -141,6 +141,10 @@ struct SegParams {
   // the position of its first head (the tile's length when it has none).
   const uint32_t* run_base;
   uint32_t* first_pos;
+  // kReduceKeysTiles: every tile's run-head bitmap (TILE / 32 words per
+  // tile), written by seg_run_heads_kernel, so the value passes need not
+  // read the keys again.
+  const uint32_t* head_bits;
 };
 
 __device__ __forceinline__ bool key_eq(int dtype, uint64_t a, uint64_t b) {
@@ -265,6 +269,13 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
       const uint64_t start = p.offsets[s];
       if (start >= tb && start < te) atomicOr(&s_bits[(start - tb) >> 5], 1u << ((start - tb) & 31));
     }
+  } else if (p.head_bits) {
+    // The heads pass left this tile's bitmap (key changes and segment
+    // starts); the next tile's first bit says whether te is a head.
+    constexpr int W = C::TILE / 32;
+    const uint32_t* hb = p.head_bits + tile * W;
+    for (int w = tid; w < W; w += kThreads) s_bits[w] = hb[w];
+    if (tid == 0) s_head_te = te < n ? (p.head_bits[(tile + 1) * W] & 1u) : 1u;
   } else {
     for (uint64_t i = tb + tid; i < te; i += kThreads) {
       bool h = i == 0;
@@ -561,7 +572,7 @@ __global__ void __launch_bounds__(kThreads)
     seg_run_heads_kernel(Src keys, uint64_t cap, const uint32_t* __restrict__ n_dev,
                          const uint32_t* __restrict__ offsets, uint64_t nseg,
                          const uint32_t* __restrict__ tile_lb, uint64_t tile_items,
-                         uint32_t* __restrict__ head_count) {
+                         uint32_t* __restrict__ head_count, uint32_t* __restrict__ head_bits) {
   constexpr int kMaxWords = 4096 / 32;  // the largest tile (4-byte values)
   __shared__ uint32_t s_bits[kMaxWords];
   __shared__ uint32_t s_cnt;
@@ -589,7 +600,10 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
   uint32_t c = 0;
-  for (int w = threadIdx.x; w < words; w += kThreads) c += __popc(s_bits[w]);
+  for (int w = threadIdx.x; w < words; w += kThreads) {
+    c += __popc(s_bits[w]);
+    head_bits[tile * words + w] = s_bits[w];
+  }
   c = __reduce_add_sync(kFull, c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_cnt, c);
   __syncthreads();
@@ -828,6 +842,7 @@ __global__ void __launch_bounds__(kThreads)
 // `tile` is the tile size they were computed for, 0 before the first).
 struct RunBases {
   uint32_t* ptr = nullptr;
+  uint32_t* bits = nullptr;  // the head bitmap: n / 32 + 256 words
   uint64_t tile = 0;
 };
 
@@ -852,10 +867,12 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
   const bool tiles_mode = p.mode == kReduceTiles || scan_tiles || keys_tiles;
   const size_t part_b = tiles_mode ? (tiles * sizeof(V) + 255) / 256 * 256 : 0;
   const size_t tseg_b = tiles_mode ? (tiles * 4 + 255) / 256 * 256 : 0;
-  // kReduceKeysTiles: run bases (tiles + 1 words) and first-head positions
+  // kReduceKeysTiles: run bases (tiles + 1 words) and first-head positions,
+  // then the head bitmap (unless shared)
   const size_t keys_b = keys_tiles ? 2 * (((tiles + 1) * 4 + 255) / 256 * 256) : 0;
+  const size_t bits_b = keys_tiles && !(rb && rb->ptr) ? (tiles + 1) * (C::TILE / 32) * 4 : 0;
   Scratch scratch;
-  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b + 2 * part_b + tseg_b + keys_b));
+  MB_TRY(scratch.alloc(ex, 256 + state_b + lb_b + 2 * part_b + tseg_b + keys_b + bits_b));
   MB_CUDA(cudaMemsetAsync(scratch.ptr, 0, 256 + state_b, ex->stream));
   p.counter = scratch.as<uint32_t>();
   p.err = DevErr{ex->status_dev, scratch.as<uint32_t>() + 1};
@@ -868,8 +885,13 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
     if (keys_tiles) {
       uint32_t* base = (uint32_t*)(q + 2 * part_b + tseg_b);
       p.first_pos = (uint32_t*)((char*)base + keys_b / 2);
-      if (rb && rb->ptr) base = rb->ptr;
+      uint32_t* bits = (uint32_t*)(q + 2 * part_b + tseg_b + keys_b);
+      if (rb && rb->ptr) {
+        base = rb->ptr;
+        bits = rb->bits;
+      }
       p.run_base = base;
+      p.head_bits = bits;
       if (!rb || rb->tile != (uint64_t)C::TILE)
         MB_CUDA(cudaMemsetAsync(base, 0, (tiles + 1) * 4, ex->stream));
     }
@@ -891,7 +913,8 @@ int seg_run(mb_executor* ex, const mb_src& in, SegParams<V> p, const void* init_
     // Every tile's first run index, and the run count.
     if (rb && rb->ptr) rb->tile = C::TILE;
     seg_run_heads_kernel<<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
-        p.keys, cap, in.len_dev, p.offsets, p.nseg, p.tile_lb, C::TILE, (uint32_t*)p.run_base);
+        p.keys, cap, in.len_dev, p.offsets, p.nseg, p.tile_lb, C::TILE, (uint32_t*)p.run_base,
+        (uint32_t*)p.head_bits);
     MB_CUDA(cudaGetLastError());
     seg_run_base_kernel<<<1, kCarryThreads, 0, ex->stream>>>(
         (uint32_t*)p.run_base, tiles, C::TILE, cap, in.len_dev, p.count_dev);
@@ -1405,8 +1428,10 @@ int mb_reduce_by_key_segmented(mb_executor* ex, const mb_src* keys, int key_eq,
       same_len = same_len && (!values[c].len_dev || values[c].len_dev == keys->len_dev);
     if (mode == kReduceKeysTiles && nvals > 1 && same_len) {
       const uint64_t min_tile = SegCfg<uint64_t>::TILE;  // 8-byte values: the smallest
-      MB_TRY(bases.alloc(ex, ((n + min_tile - 1) / min_tile + 1) * 4));
+      const uint64_t base_words = ((n + min_tile - 1) / min_tile + 1 + 63) / 64 * 64;
+      MB_TRY(bases.alloc(ex, (base_words + n / 32 + 256) * 4));
       rb.ptr = bases.as<uint32_t>();
+      rb.bits = rb.ptr + base_words;
     }
     for (int c = 0; c < nvals; ++c) {
       // The keys' device length (a count left by an earlier step) bounds
