@@ -99,7 +99,8 @@ __device__ __forceinline__ uint32_t ss_load(const Src& in, uint64_t i) {
 }
 
 // Exclusive scan of one value per thread (kSsThreads of them) in thread
-// order.  Uses sm.wsum; ends with a barrier.
+// order.  Uses sm.wsum, which every caller leaves alone until its next block
+// barrier (so no barrier is needed after the reads here).
 template <bool PAY>
 __device__ __forceinline__ uint32_t ss_block_excl(SsSmem<PAY>& sm, uint32_t v) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -113,7 +114,6 @@ __device__ __forceinline__ uint32_t ss_block_excl(SsSmem<PAY>& sm, uint32_t v) {
   __syncthreads();
   uint32_t ex = incl - v;
   for (int w = 0; w < warp; ++w) ex += sm.wsum[w];
-  __syncthreads();  // wsum is free again
   return ex;
 }
 
@@ -200,10 +200,100 @@ __device__ __forceinline__ void ss_pass(SsSmem<PAY>& sm, uint32_t valid, int shi
   __syncthreads();
 }
 
+// After passes that left out the value bits `low` (the lowest varying
+// digits), the keys are in order of (segment, value without `low`), equal
+// ones in input order.  Sorts each run of keys equal there by the whole
+// value: runs already in order are left as they are, runs of at most
+// kSsFixRun keys that are not get a stable insertion sort by one thread.
+// Returns false, with the keys in an unknown order, when a longer run is out
+// of order (the caller then sorts the pack again with every digit).  Uses
+// sm.hist for the run bitmap and the mask tables for run starts and flags,
+// and leaves the mask tables zero.
+constexpr uint32_t kSsFixRun = 32;
+
+template <bool PAY>
+__device__ bool ss_fix_runs(SsSmem<PAY>& sm, uint32_t len, uint32_t low) {
+  const int tid = threadIdx.x;
+  const uint64_t hmask = ~(uint64_t)low;
+  uint32_t* rheads = sm.hist[0];  // kSsTile / 32 words: run starts
+  uint32_t* rpre = sm.hist[1];    // runs before each word
+  uint16_t* rstart = reinterpret_cast<uint16_t*>(&sm.mask[0][0][0]);  // kSsTile + 1 entries
+  uint32_t* rflag = &sm.mask[2][0][0];  // kSsTile bits: the run is out of order
+  static_assert(2 * sizeof(sm.mask[0]) >= (kSsTile + 1) * sizeof(uint16_t),
+                "run starts fit the first two mask tables");
+  if (tid < kSsTile / 32) {
+    rheads[tid] = 0;
+    rflag[tid] = 0;
+  }
+  if (tid == 0) sm.flag[0] = 0;
+  __syncthreads();
+  bool any = false;  // a key below the one before it in the same run
+  for (uint32_t b = 0; b < len; b += kSsThreads) {  // a warp's 32 positions form one word
+    const uint32_t p = b + tid;
+    bool head = false;
+    if (p < len) {
+      const uint64_t k = sm.keys[p];
+      const uint64_t q = p ? sm.keys[p - 1] : 0ull;
+      head = p == 0 || ((q ^ k) & hmask) != 0;
+      any |= !head && (uint32_t)q > (uint32_t)k;
+    }
+    const uint32_t word = __ballot_sync(kFull, head);
+    if ((tid & 31) == 0) rheads[p >> 5] = word;
+  }
+  if (__syncthreads_or(any) == 0) return true;  // no run out of order
+  {
+    const uint32_t c = tid < kSsTile / 32 ? (uint32_t)__popc(rheads[tid]) : 0u;
+    const uint32_t ex = ss_block_excl(sm, c);
+    if (tid < kSsTile / 32) rpre[tid] = ex;
+  }
+  __syncthreads();
+  const uint32_t runs = rpre[kSsTile / 32 - 1] + (uint32_t)__popc(rheads[kSsTile / 32 - 1]);
+  for (uint32_t p = tid; p < len; p += kSsThreads) {
+    const uint32_t w = p >> 5;
+    const bool head = (rheads[w] >> (p & 31)) & 1u;
+    const uint32_t r =
+        rpre[w] + (uint32_t)__popc(rheads[w] & (0xFFFFFFFFu >> (31 - (p & 31)))) - 1u;
+    if (head) rstart[r] = (uint16_t)p;
+    else if ((uint32_t)sm.keys[p - 1] > (uint32_t)sm.keys[p])
+      atomicOr(&rflag[r >> 5], 1u << (r & 31));
+  }
+  if (tid == 0) rstart[runs] = (uint16_t)len;
+  __syncthreads();
+  for (uint32_t r = tid; r < runs; r += kSsThreads) {
+    if (!((rflag[r >> 5] >> (r & 31)) & 1u)) continue;
+    const uint32_t a = rstart[r], b = rstart[r + 1];
+    if (b - a > kSsFixRun) {
+      sm.flag[0] = 1;
+      continue;
+    }
+    for (uint32_t i = a + 1; i < b; ++i) {  // stable: only strictly greater keys move
+      const uint64_t k = sm.keys[i];
+      uint32_t pv = 0;
+      if constexpr (PAY) pv = sm.pay[i];
+      uint32_t j = i;
+      while (j > a && (uint32_t)sm.keys[j - 1] > (uint32_t)k) {
+        sm.keys[j] = sm.keys[j - 1];
+        if constexpr (PAY) sm.pay[j] = sm.pay[j - 1];
+        --j;
+      }
+      sm.keys[j] = k;
+      if constexpr (PAY) sm.pay[j] = pv;
+    }
+  }
+  __syncthreads();
+  const bool ok = sm.flag[0] == 0;
+  // Back to zero: the words that held run starts and flags.
+  uint32_t* m0 = &sm.mask[0][0][0];
+  for (int i = tid; i < (kSsTile + 2) / 2; i += kSsThreads) m0[i] = 0;
+  if (tid < kSsTile / 32) rflag[tid] = 0;
+  __syncthreads();
+  return ok;
+}
+
 // Sorts the pack of segments [s_begin, s_end) (items [start, start + len),
 // len < kSsTile, start = offsets[s_begin]) into out.
 template <int ENC, bool PAY, bool PLAIN>
-__device__ void ss_pack(SsSmem<PAY>& sm, const Src& in, const uint32_t* __restrict__ off,
+__device__ __forceinline__ void ss_pack(SsSmem<PAY>& sm, const Src& in, const uint32_t* __restrict__ off,
                         uint64_t s_begin, uint64_t s_end, uint32_t start, uint32_t len, int desc,
                         int ieee, uint32_t* __restrict__ out) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -274,9 +364,39 @@ __device__ void ss_pack(SsSmem<PAY>& sm, const Src& in, const uint32_t* __restri
     var_lo = a ^ b;  // bits that differ between some two items
     var_hi = c ^ e;
   }
-  for (int shift = 0; shift < 64; shift += 8) {
-    const uint32_t v = shift < 32 ? (var_lo >> shift) : (var_hi >> (shift - 32));
-    if (v & 0xFFu) ss_pass(sm, len, shift);
+  // The lowest of four varying value digits is left out of the passes
+  // (`low`): a pack's keys rarely agree on segment and the value's top three
+  // digits, and ss_fix_runs orders the few that do.  (Leaving out two digits
+  // saved a pass but made runs common enough that their fix-up cost more.)
+  uint32_t low = 0;
+  {
+    int m = 0, c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) m += ((var_lo >> (8 * j)) & 0xFFu) != 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (((var_lo >> (8 * j)) & 0xFFu) && ++c == m - 3)
+        low = j == 3 ? ~0u : ((1u << (8 * j + 8)) - 1u);
+  }
+  auto passes = [&](uint32_t vlo) {
+    for (int shift = 0; shift < 64; shift += 8) {
+      const uint32_t v = shift < 32 ? (vlo >> shift) : (var_hi >> (shift - 32));
+      if (v & 0xFFu) ss_pass(sm, len, shift);
+    }
+  };
+  passes(var_lo & ~low);
+  if (low && !ss_fix_runs(sm, len, low)) {
+    // A long run out of order: build the keys again and take every digit.
+    for (uint32_t p = tid; p < len; p += kSsThreads) {
+      const uint32_t r = ss_load<PLAIN>(in, (uint64_t)start + p);
+      const uint32_t w = p >> 5;
+      const uint32_t seg =
+          sm.hpre[w] + (uint32_t)__popc(sm.heads[w] & (0xFFFFFFFFu >> (31 - (p & 31)))) - 1u;
+      sm.keys[p] = ((uint64_t)seg << 32) | ss_encode<ENC>(r, desc, ieee);
+      if constexpr (PAY) sm.pay[p] = r;
+    }
+    __syncthreads();
+    passes(var_lo);
   }
   for (uint32_t p = tid; p < len; p += kSsThreads) {
     uint32_t v;

@@ -171,3 +171,30 @@ def test_graph_capture_replays(ex):
         torch.cuda.synchronize()
         assert np.array_equal(ex.to_host(cap.outputs), want)
     cap.release()
+
+
+@pytest.mark.parametrize("less", ["less", "greater"])
+def test_runs_equal_in_the_high_digits(ex, less):
+    # The passes leave out the lowest varying digits and order the runs of
+    # keys that agree on the rest afterwards: short runs out of order, long
+    # runs already in order (duplicates), and long runs out of order (the
+    # whole pack sorted again with every digit).
+    n = 40_000
+    u = seeded(np.uint32, n, 13)
+    lens = [1500, 2000, 300, 4000, 20_000, 2100, 10_100]
+    off = _offsets(lens)
+    # every digit varies, the top three from one bit each, the lowest is
+    # random: keys agree on the top three digits in long runs
+    x = ((u >> 31) << 24) | (((u >> 30) & 1) << 16) | (((u >> 29) & 1) << 8) | (u & 0xFF)
+    x = x.astype(np.uint32)
+    # a stretch of one repeated value (a long run in order)
+    x[1500:3000] = 0x12345678
+    # a stretch of full-range values (runs of two or three, rarely)
+    x[3500:3800] = seeded(np.uint32, 300, 14)
+    x[30_000:40_000] = seeded(np.uint32, 10_000, 15)
+    got = _run(ex, x, off, less)
+    assert np.array_equal(got, orc.seg_sort(x, off, less))
+    f = (x.view(np.float32) * np.float32(1)).astype(np.float32)
+    f[np.isnan(f)] = np.float32(-0.0)
+    got = _run(ex, f, off, less)
+    assert np.array_equal(got.view(np.uint32), orc.seg_sort(f, off, less).view(np.uint32))
