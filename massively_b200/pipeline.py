@@ -87,3 +87,67 @@ class Captured:
         self.graph = None
         self.outputs = None
         self.arena = None
+
+
+def run_host_batches(exec: Executor, fn, batches, outs) -> None:
+    """Runs `fn(exec, *device_inputs) -> DeviceVec` over a sequence of host
+    batches, with the copies overlapped: batch i + 1 uploads and batch i - 1
+    downloads while the kernels of batch i run.
+
+    `batches[i]` is a tuple of pinned host arrays (the same shapes and types
+    for every batch); the result of batch i is copied into the pinned host
+    array `outs[i]` (all of its elements, so `fn` should not leave a device
+    length on it).  Uploads, kernels and downloads run on three streams of the
+    executor's device, with two sets of device input buffers used in turn: a
+    set is refilled only after the kernels that read it have finished.  The
+    outputs of one call land in order on the download stream, so `outs` may
+    repeat arrays (the last batch written wins).  Returns once every result
+    is on the host; the executor is then bound to the caller's stream again.
+    massively uploads, runs and downloads one batch at a time; this is for
+    callers that stream many host batches through one device."""
+    from .runtime import NP_TO_TORCH
+    if not batches:
+        return
+    dev = exec.device
+    caller = torch.cuda.current_stream(dev)
+    up, comp, down = (torch.cuda.Stream(dev) for _ in range(3))
+    slots = [[torch.empty(h.size, dtype=NP_TO_TORCH[h.dtype], device=f"cuda:{dev}")
+              for h in batches[0]] for _ in range(2)]
+    free = []
+    for _ in range(2):
+        e = torch.cuda.Event()
+        e.record(caller)
+        free.append(e)
+    for s in (up, comp, down):
+        s.wait_stream(caller)
+    try:
+        for i, batch in enumerate(batches):
+            k = i % 2
+            up.wait_event(free[k])
+            with torch.cuda.stream(up):
+                for t, h in zip(slots[k], batch):
+                    if h.size != t.numel() or NP_TO_TORCH[h.dtype] != t.dtype:
+                        raise ValueError("every batch has the first one's shapes and types")
+                    src = torch.from_numpy(h.reshape(-1).view(np.uint8)).view(t.dtype)
+                    t.copy_(src, non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(up)
+            comp.wait_event(ready)
+            with torch.cuda.stream(comp):
+                exec.bind_current_stream()
+                res = fn(exec, *[DeviceVec(exec, t) for t in slots[k]])
+                done = torch.cuda.Event()
+                done.record(comp)
+            free[k] = done
+            down.wait_event(done)
+            with torch.cuda.stream(down):
+                r = res.tensor
+                dst = torch.from_numpy(outs[i].reshape(-1).view(np.uint8)).view(r.dtype)
+                dst[:r.numel()].copy_(r, non_blocking=True)
+                r.record_stream(down)
+        down.synchronize()
+    finally:
+        with torch.cuda.stream(caller):
+            exec.bind_current_stream()
+        caller.wait_stream(down)
+        caller.wait_stream(comp)
