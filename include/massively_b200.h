@@ -551,7 +551,8 @@ enum {
   MB_TUNE_RADIX = 1,
   MB_TUNE_REDUCE = 2,
   MB_TUNE_SELECT = 3,
-  MB_TUNE_SEG = 4 /* ForEachSegment(Reduce): tile-local folds or a carried look-back */
+  MB_TUNE_SEG = 4, /* ForEachSegment(Reduce): tile-local folds or a carried look-back */
+  MB_TUNE_SEARCH = 5 /* lower_bound / upper_bound: line levels or a two-level binary search */
 };
 int mb_tune_config_count(int family);
 int mb_tune_set(mb_executor* exec, int family, int config);

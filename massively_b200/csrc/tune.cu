@@ -18,6 +18,7 @@ int mb_tune_config_count(int family) {
     case MB_TUNE_RADIX: return radix_tune_count();
     case MB_TUNE_SCAN: return 3;
     case MB_TUNE_SEG: return 2;
+    case MB_TUNE_SEARCH: return 2;
     case MB_TUNE_REDUCE: case MB_TUNE_SELECT: return 1;
     default: return 0;
   }
@@ -34,6 +35,12 @@ const char* mb_tune_describe(int family, int config) {
            "segments crossing tiles";
   if (family == MB_TUNE_SEG && config == 1)
     return "segmented scan / reduce over offsets: a decoupled look-back carried across tiles";
+  if (family == MB_TUNE_SEARCH && config == 0)
+    return "bounds search by 128-byte lines: a sample level per 32 (u32) elements, the top "
+           "level in shared memory";
+  if (family == MB_TUNE_SEARCH && config == 1)
+    return "bounds search: binary search over 16 KB of samples in shared memory, then over "
+           "the source interval";
   if (config == 0) {
     switch (family) {
       case MB_TUNE_SCAN: return "scan one 32 KB tile per CTA, a ninth warp runs the look-back";

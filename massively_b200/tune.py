@@ -33,7 +33,7 @@ import numpy as np
 from . import _native as N
 from .runtime import check
 
-FAMILIES = {"scan": 0, "radix": 1, "reduce": 2, "select": 3, "seg": 4}
+FAMILIES = {"scan": 0, "radix": 1, "reduce": 2, "select": 3, "seg": 4, "search": 5}
 
 
 def default_db_path() -> str:

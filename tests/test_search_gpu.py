@@ -105,3 +105,38 @@ def test_unique_and_by_key(ex, n, dtype):
     a, b = got.cols
     np.testing.assert_array_equal(ex.to_host(a), vals[heads])
     np.testing.assert_array_equal(ex.to_host(b), x[heads])
+
+
+@pytest.mark.parametrize("dtype,n", [(np.uint32, 16_383), (np.uint32, 16_384), (np.uint32, 524_289),
+                                     (np.uint32, (1 << 24) + 3), (np.int64, 131_073),
+                                     (np.float64, 2_100_000), (np.float32, 600_000)])
+def test_search_by_lines_levels(ex, dtype, n):
+    # Sources that need from zero to seven line levels below the
+    # shared-memory tree (its size just under and over a complete tree), with
+    # partial last lines, against the oracle; an unaligned slice of the same
+    # source takes the two-level binary search and must agree; so must the
+    # binary search chosen through the tuner.
+    from massively_b200 import tune, vector
+    rng = np.random.default_rng(n)
+    if np.dtype(dtype).kind == "f":
+        src = np.sort(rng.normal(size=n).astype(dtype))
+        vals = rng.normal(size=50_000).astype(dtype)
+        vals[:100] = src[rng.integers(0, n, 100)]
+        vals[100] = src[0]
+        vals[101] = src[-1]
+    else:
+        src = np.sort(rng.integers(0, 1 << 20, n).astype(dtype))  # many duplicates
+        vals = rng.integers(0, (1 << 20) + 5, 50_000).astype(dtype)
+    ds, dv = ex.to_device(src), ex.to_device(vals)
+    lo = ex.to_host(vector.lower_bound(ex, ds, dv))
+    hi = ex.to_host(vector.upper_bound(ex, ds, dv))
+    np.testing.assert_array_equal(lo, orc.lower_bound(src, vals))
+    np.testing.assert_array_equal(hi, orc.upper_bound(src, vals))
+    sl = ds.slice(1, n)
+    np.testing.assert_array_equal(ex.to_host(vector.lower_bound(ex, sl, dv)),
+                                  orc.lower_bound(src[1:], vals))
+    tune.set_config(ex, "search", 1)
+    try:
+        np.testing.assert_array_equal(ex.to_host(vector.upper_bound(ex, ds, dv)), hi)
+    finally:
+        tune.set_config(ex, "search", -1)
