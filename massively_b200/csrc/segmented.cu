@@ -238,6 +238,25 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
                                                       (uint64_t)(j * 32 + lane) * VEC));
       memcpy(raw[j], &u, 16);
     }
+  } else if (!PLAIN && full && in.kind == MB_SRC_COLUMN && (uintptr_t)in.data % 16 == 0 &&
+             (sizeof(V) == 4 ? (in.dtype == MB_U32 || in.dtype == MB_I32 || in.dtype == MB_F32)
+                             : (in.dtype == MB_U64 || in.dtype == MB_I64 || in.dtype == MB_F64))) {
+    // A mapped or cast column of V's width (a predicate's 0 / 1 flags for
+    // count_if, say): the same 16-byte loads, the map applied per element.
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      uint4 u = __ldcs(reinterpret_cast<const uint4*>(
+          (const char*)in.data + (warp_base + (uint64_t)(j * 32 + lane) * VEC) * sizeof(V)));
+      if constexpr (sizeof(V) == 4) {
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) raw[j][k] = map_to<V>(in.map, in.dtype, w[k]);
+      } else {
+        const uint64_t w[2] = {((uint64_t)u.y << 32) | u.x, ((uint64_t)u.w << 32) | u.z};
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) raw[j][k] = map_to<V>(in.map, in.dtype, w[k]);
+      }
+    }
   } else {
 #pragma unroll
     for (int j = 0; j < kLoads; ++j)
