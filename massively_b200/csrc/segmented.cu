@@ -257,6 +257,14 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
         for (int k = 0; k < VEC; ++k) raw[j][k] = map_to<V>(in.map, in.dtype, w[k]);
       }
     }
+  } else if (!PLAIN && in.kind == MB_SRC_CONSTANT) {
+    // A constant column (the count of a group-by): one value, no loads.
+    const V c = src_load<V>(in, 0);
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+      for (int k = 0; k < VEC; ++k)
+        raw[j][k] = warp_base + (uint64_t)(j * 32 + lane) * VEC + k < n ? c : V(0);
   } else {
 #pragma unroll
     for (int j = 0; j < kLoads; ++j)
