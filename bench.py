@@ -925,7 +925,7 @@ def run_ours(args):
     if not args.no_e2e:
         try:
             torch.cuda.empty_cache()
-            e2e = e2e_measure(ex, WORKLOADS[args.workload](), max(2, min(args.steps, 8)))
+            e2e = e2e_measure(ex, WORKLOADS[args.workload](), max(2, min(args.steps, 16)))
         except Exception as e:
             e2e = {"error": str(e)[:200]}
     cpu = None
