@@ -612,10 +612,25 @@ __global__ void __launch_bounds__(kThreads)
   for (int w = threadIdx.x; w < words; w += kThreads) s_bits[w] = 0;
   if (threadIdx.x == 0) s_cnt = 0;
   __syncthreads();
-  for (uint64_t i = tb + threadIdx.x; i < te; i += kThreads) {
-    bool h = i == 0;
-    if (!h) h = !key_eq(keys.vtype, src_load_bits(keys, i - 1), src_load_bits(keys, i));
-    if (h) atomicOr(&s_bits[(i - tb) >> 5], 1u << ((i - tb) & 31));
+  // A warp's 32 lanes take 32 consecutive items: one ballot is one bitmap
+  // word.  Plain 4-byte keys are read directly (the item before comes from
+  // the same or the previous line).
+  const bool plain4 = keys.kind == MB_SRC_COLUMN && keys.map == MB_UN_IDENTITY &&
+                      keys.dtype == keys.vtype &&
+                      (keys.dtype == MB_U32 || keys.dtype == MB_I32 || keys.dtype == MB_F32);
+  const uint32_t* kp = (const uint32_t*)keys.data;
+  for (uint64_t b = tb; b < te; b += kThreads) {
+    const uint64_t i = b + threadIdx.x;
+    bool h = false;
+    if (i < te) {
+      h = i == 0;
+      if (!h) {
+        if (plain4) h = !key_eq(keys.vtype, __ldg(kp + i - 1), __ldg(kp + i));
+        else h = !key_eq(keys.vtype, src_load_bits(keys, i - 1), src_load_bits(keys, i));
+      }
+    }
+    const uint32_t word = __ballot_sync(kFull, h);
+    if ((threadIdx.x & 31) == 0 && word) atomicOr(&s_bits[(i - tb) >> 5], word);
   }
   if (offsets) {
     const uint64_t sa = tile_lb[tile];
@@ -744,6 +759,56 @@ __global__ void __launch_bounds__(kCarryThreads)
   // The last run, when no head in the last tile let that tile write it.
   if (u0 < u1 && u1 == live && !prev_head)
     st_cast<V>(out_dtype, out, run_base[live] - 1, op_apply_rt<V>(op, init, run.v));
+}
+
+// reduce_by_key of a constant integer column under ADD: every run's value is
+// init + c * (its length), so no value pass is needed.  seg_run_starts_kernel
+// turns the call's run-head bitmap (tiles of `tile_items`) and run bases into
+// each run's first position, one block per tile; seg_const_runs_kernel writes
+// the values.  Integer adds wrap, so c * length equals the repeated adds.
+__global__ void __launch_bounds__(kThreads)
+    seg_run_starts_kernel(const uint32_t* __restrict__ head_bits,
+                          const uint32_t* __restrict__ run_base, uint64_t tile_items,
+                          uint64_t cap, const uint32_t* __restrict__ n_dev,
+                          uint32_t* __restrict__ starts) {
+  __shared__ uint32_t s_wsum[kWarps];
+  const uint64_t tile = blockIdx.x;
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t tb = tile * tile_items;
+  if (tb >= n) return;
+  const int words = (int)(tile_items / 32);  // at most kThreads
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t w = (int)threadIdx.x < words ? head_bits[tile * words + threadIdx.x] : 0u;
+  const uint32_t c = (uint32_t)__popc(w);
+  uint32_t incl = c;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(kFull, incl, d);
+    if (lane >= d) incl += o;
+  }
+  if (lane == 31) s_wsum[warp] = incl;
+  __syncthreads();
+  uint32_t r = run_base[tile] + incl - c;
+  for (int v = 0; v < warp; ++v) r += s_wsum[v];
+  for (uint32_t bits = w; bits; bits &= bits - 1)
+    starts[r++] = (uint32_t)(tb + threadIdx.x * 32u + (uint32_t)(__ffs(bits) - 1));
+}
+
+template <class V>
+__global__ void __launch_bounds__(kThreads)
+    seg_const_runs_kernel(const uint32_t* __restrict__ starts,
+                          const uint32_t* __restrict__ run_base, uint64_t tile_items,
+                          uint64_t cap, const uint32_t* __restrict__ n_dev, V init, V value,
+                          void* out, int out_dtype) {
+  using U = typename std::make_unsigned<V>::type;
+  const uint64_t n = n_dev ? min((uint64_t)*n_dev, cap) : cap;
+  const uint64_t runs = run_base[(n + tile_items - 1) / tile_items];
+  for (uint64_t r = blockIdx.x * (uint64_t)kThreads + threadIdx.x; r < runs;
+       r += (uint64_t)gridDim.x * kThreads) {
+    const uint64_t end = r + 1 < runs ? (uint64_t)starts[r + 1] : n;
+    const U len = (U)(end - starts[r]);
+    st_cast<V>(out_dtype, out, r, (V)((U)init + (U)value * len));
+  }
 }
 
 // Whether tile t (items [t * tile_items, te)) holds a segment start: the
@@ -1460,15 +1525,56 @@ int mb_reduce_by_key_segmented(mb_executor* ex, const mb_src* keys, int key_eq,
       rb.ptr = bases.as<uint32_t>();
       rb.bits = rb.ptr + base_words;
     }
-    for (int c = 0; c < nvals; ++c) {
+    // A constant integer column under ADD (a group-by's count) needs no
+    // value pass once the run heads are known: its runs are init + c * length.
+    auto counts_runs = [&](int c) {
+      const mb_src& v = values[c];
+      return rb.ptr && v.kind == MB_SRC_CONSTANT && v.map == MB_UN_IDENTITY &&
+             v.dtype == v.vtype && ops[c] == MB_OP_ADD &&
+             (v.dtype == MB_U32 || v.dtype == MB_I32 || v.dtype == MB_U64 || v.dtype == MB_I64);
+    };
+    int primary = 0;  // writes the keys and the run count
+    while (primary < nvals && counts_runs(primary)) ++primary;
+    if (primary == nvals) primary = 0;
+    bool any_const = false;
+    for (int k = 0; k < nvals; ++k) {
+      const int c = k == 0 ? primary : (k <= primary ? k - 1 : k);
+      if (c != primary && counts_runs(c)) {
+        any_const = true;
+        continue;
+      }
       // The keys' device length (a count left by an earlier step) bounds
       // value views that carry none, such as a constant column.
       mb_src v = values[c];
       if (!v.len_dev) v.len_dev = keys->len_dev;
       MB_TRY(seg_entry(ex, &v, ops[c], mode, &inits[c], out_values[c].data,
                        out_values[c].dtype, offsets, segment_count, keys,
-                       c == 0 ? out_keys.data : nullptr,
-                       (int)dtype_size(out_keys.dtype), c == 0 ? count_dev : nullptr, &rb));
+                       c == primary ? out_keys.data : nullptr,
+                       (int)dtype_size(out_keys.dtype), c == primary ? count_dev : nullptr, &rb));
+    }
+    if (any_const) {
+      const uint64_t tiles = (n + rb.tile - 1) / rb.tile;
+      Scratch starts;
+      MB_TRY(starts.alloc(ex, n * 4));
+      seg_run_starts_kernel<<<(unsigned)tiles, kThreads, 0, ex->stream>>>(
+          rb.bits, rb.ptr, rb.tile, n, keys->len_dev, starts.as<uint32_t>());
+      MB_CUDA(cudaGetLastError());
+      const unsigned g = (unsigned)std::min<uint64_t>((n + kThreads - 1) / kThreads, 148ull * 8);
+      for (int c = 0; c < nvals; ++c) {
+        if (c == primary || !counts_runs(c)) continue;
+        const mb_src& v = values[c];
+        if (dtype_size(v.dtype) == 4) {
+          const uint32_t init = (uint32_t)inits[c], val = (uint32_t)v.a;
+          seg_const_runs_kernel<uint32_t><<<g, kThreads, 0, ex->stream>>>(
+              starts.as<uint32_t>(), rb.ptr, rb.tile, n, keys->len_dev, init, val,
+              out_values[c].data, out_values[c].dtype);
+        } else {
+          seg_const_runs_kernel<uint64_t><<<g, kThreads, 0, ex->stream>>>(
+              starts.as<uint32_t>(), rb.ptr, rb.tile, n, keys->len_dev, (uint64_t)inits[c],
+              (uint64_t)v.a, out_values[c].data, out_values[c].dtype);
+        }
+        MB_CUDA(cudaGetLastError());
+      }
     }
   }
   if (count_host) MB_TRY(read_u32(ex, count_dev, count_host));

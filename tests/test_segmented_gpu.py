@@ -245,3 +245,43 @@ def test_group_by_columns(ex):
     np.testing.assert_array_equal(ex.to_host(m), wm)
     abs_sum = orc.reduce_by_key(keys, np.abs(vals.astype(np.float64)), "add", 0.0)[1]
     assert (np.abs(ex.to_host(s) - ws) <= wc * 2.0 ** -24 * abs_sum + 1e-30).all()
+
+
+@pytest.mark.parametrize("n", [1, 4095, 4097, 70_001, 1 << 20])
+def test_constant_columns_count_runs(ex, n):
+    # Constant integer columns under ADD come from the run lengths (no value
+    # pass): first in the zip (another column writes the keys), 64-bit, signed
+    # with a negative constant, beside a plain column and a non-ADD constant;
+    # and the segmented form, whose runs also break at segment starts.
+    from massively_b200 import lazy, op, vector, zip4
+    keys = np.sort((seeded(np.uint32, n, 7) % max(1, n // 37)).astype(np.uint32))
+    vals = (seeded(np.uint32, n, 8) % 1000).astype(np.uint32)
+    dk, dv = ex.to_device(keys), ex.to_device(vals)
+    cols = zip4(lazy.constant(np.uint32(3)).take(n), dv, lazy.constant(np.int64(-2)).take(n),
+                lazy.constant(np.uint32(5)).take(n))
+    inits = (np.uint32(7), np.uint32(0), np.int64(11), np.uint32(9))
+    ops = (op.Add, op.Add, op.Add, op.Max)
+    ok, ov = vector.reduce_by_key(ex, dk, cols, op.Equal, inits, ops)
+    a, b, c, d = (ex.to_host(x) for x in ov.into_columns())
+    wk, (wa, wb, wc, wd) = orc.reduce_by_key(
+        keys, [np.full(n, 3, np.uint32), vals, np.full(n, -2, np.int64), np.full(n, 5, np.uint32)],
+        ["add", "add", "add", "max"], [7, 0, 11, 9])
+    np.testing.assert_array_equal(ex.to_host(ok), wk)
+    for got, want in ((a, wa), (b, wb), (c, wc), (d, wd)):
+        np.testing.assert_array_equal(got, want)
+    # segmented: segment starts every 1000 items also end runs
+    off = np.arange(0, n + 1000, 1000, dtype=np.uint32)
+    off[-1] = n
+    off = np.unique(np.minimum(off, n)).astype(np.uint32)
+    sk, sv = vector.reduce_by_key_segmented(ex, dk, cols, op.Equal, inits, ops, ex.to_device(off))
+    heads = np.ones(n, bool)
+    heads[1:] = keys[1:] != keys[:-1]
+    heads[off[:-1]] = True
+    starts = np.flatnonzero(heads)
+    lens = np.diff(np.append(starts, n)).astype(np.uint64)
+    np.testing.assert_array_equal(ex.to_host(sk), keys[starts])
+    sa, sb, sc, sd = (ex.to_host(x) for x in sv.into_columns())
+    np.testing.assert_array_equal(sa, (7 + 3 * lens).astype(np.uint32))
+    np.testing.assert_array_equal(sc, (11 - 2 * lens.astype(np.int64)).astype(np.int64))
+    np.testing.assert_array_equal(sb, np.add.reduceat(vals.astype(np.uint64), starts).astype(np.uint32))
+    np.testing.assert_array_equal(sd, np.full(starts.size, 9, np.uint32))
