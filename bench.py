@@ -883,6 +883,9 @@ def run_ours(args):
         for name in SECONDARY:
             try:
                 w2 = WORKLOADS[name]()
+                # this workload's recorded tuning (the caller's database, then
+                # the shipped table), else the built-in defaults
+                ch2 = tune.apply(ex, w2.dtype, getattr(w2, "n", None))
                 w2.setup(ex)
                 kt2 = {}
                 st2 = max(3, args.steps)
@@ -896,10 +899,15 @@ def run_ours(args):
                                    "kernel": w2.kernel, "kernel_achieved_gbs": a2,
                                    "roofline_frac": a2 / peak,
                                    "step_achieved_gbs": w2.alg_bytes() / (ms2 * 1e-3) / 1e9}
+                tuned = {f: {"config": c, "source": s} for f, (c, s) in ch2.items()
+                         if s != "default"}
+                if tuned:
+                    secondary[name]["tuning"] = tuned
                 del w2
                 torch.cuda.empty_cache()
             except Exception as e:  # a secondary that is not built yet
                 secondary[name] = {"error": str(e)[:200]}
+        tune.apply(ex, wl.dtype, wl.n)  # back to the headline's choices
         # the serving loop on a shortened trace (MB_SERVE_SECONDS s of arrivals)
         try:
             torch.cuda.empty_cache()

@@ -18,7 +18,9 @@ work -- a segment-length class: log2 of the mean length and the coefficient
 of variation rounded to a half).  `apply()` selects the recorded choices for
 a workload on an executor and returns them.  The database lives outside the
 package (MB_TUNE_DB, else $XDG_CACHE_HOME/massively_b200/tune_db.json, else
-~/.cache/massively_b200/tune_db.json).  Environment variables MB_TUNE_SCAN,
+~/.cache/massively_b200/tune_db.json).  Keys missing there fall back to a
+read-only table shipped with the package (tune_table.json: choices measured
+on a B200 for the benchmark's workloads, under the device name "*").  Environment variables MB_TUNE_SCAN,
 MB_TUNE_RADIX, MB_TUNE_REDUCE, MB_TUNE_SELECT and MB_TUNE_SEG force a
 configuration.
 """
@@ -125,17 +127,23 @@ def autotune(exec, family: str, dtype: str, n: int, run, reps: int = 5, warmup: 
     return best
 
 
+SHIPPED_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tune_table.json")
+
+
 def lookup(device_name: str, family: str, dtype: str, n: int, path: str | None = None,
-           dist: str = ""):
+           dist: str = "", shipped: bool = False):
     rec = load_db(path).get(_key(device_name, family, dtype, n, dist))
+    if rec is None and shipped:
+        rec = load_db(SHIPPED_TABLE).get(_key("*", family, dtype, n, dist))
     return None if rec is None else int(rec["config"])
 
 
 def apply(exec, dtype: str | None = None, n: int | None = None, path: str | None = None,
           dist: str = "") -> dict:
     """Selects, per family, an environment override, else the recorded
-    choice for (dtype, n, dist), else the built-in default; returns
-    {family: (config, source)} with source "env", "db" or "default"."""
+    choice for (dtype, n, dist) -- the caller's database, then the shipped
+    table -- else the built-in default; returns {family: (config, source)}
+    with source "env", "db", "shipped" or "default"."""
     chosen = {}
     name = None
     for fam, fid in FAMILIES.items():
@@ -150,9 +158,14 @@ def apply(exec, dtype: str | None = None, n: int | None = None, path: str | None
                 import torch
                 name = torch.cuda.get_device_name(exec.device)
             c = lookup(name, fam, dtype, n, path, dist)
+            if c is None:
+                c = lookup(name, fam, dtype, n, path, dist, shipped=True)
+                src = "shipped"
+            else:
+                src = "db"
         if c is not None:
             set_config(exec, fam, c)
-            chosen[fam] = (c, "db")
+            chosen[fam] = (c, src)
         else:
             set_config(exec, fam, -1)
             chosen[fam] = (-1, "default")

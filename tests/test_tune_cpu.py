@@ -57,3 +57,18 @@ def test_segment_length_class_keys_records():
     assert tune.segment_class([]) == ""
     assert tune._key("D", "seg", "f32", 1 << 26, even) == "D|seg|f32|2^26|seg:mean2^6:cv0"
     assert tune._key("D", "radix", "u32", 1 << 26) == "D|radix|u32|2^26"
+
+
+def test_shipped_table_backs_the_database(tmp_path):
+    # A key the caller's database lacks falls back to the table shipped with
+    # the package (device "*"); the caller's own record wins over it.
+    path = str(tmp_path / "db.json")
+    assert tune.lookup("NVIDIA B200", "radix", "u32/f32", 1 << 27, path) is None
+    assert tune.lookup("NVIDIA B200", "radix", "u32/f32", 1 << 27, path, shipped=True) == 9
+    key = tune._key("NVIDIA B200", "radix", "u32/f32", 1 << 27)
+    tune.save_db({key: {"config": 2, "ms": 1.0}}, path)
+    assert tune.lookup("NVIDIA B200", "radix", "u32/f32", 1 << 27, path, shipped=True) == 2
+    shipped = json.load(open(tune.SHIPPED_TABLE))
+    for k, rec in shipped.items():
+        fam = k.split("|")[1]
+        assert 0 <= rec["config"] < len(tune.configs(fam))
