@@ -513,24 +513,39 @@ __global__ void __launch_bounds__(kThreads, kSegMinBlocks)
     // kReduceKeysTiles: run index = the tile's first run index + the tile-
     // local inclusive head count - 1.  Items before the tile's first head
     // belong to the run that came in from an earlier tile.
+    // One thread per bitmap word visits only its heads (the keys) and its
+    // tails (items followed by a head; the tile's last item when the item
+    // after the tile is one): runs are usually far fewer than items.
     const uint32_t base = p.run_base[tile];
-    for (uint64_t i = tb + tid; i < te; i += kThreads) {
-      const uint32_t pos = (uint32_t)(i - tb);
-      const T yv = stage[pos];
-      const bool head = (s_bits[pos >> 5] >> (pos & 31)) & 1u;
-      if (head && p.out_keys)
-        st_raw_bits(p.out_keys, base + yv.heads - 1, p.out_key_esize, src_load_bits(p.keys, i));
-      const bool last = i + 1 == te;
-      const bool tail = last ? (s_head_te != 0)
-                             : (((s_bits[(pos + 1) >> 5] >> ((pos + 1) & 31)) & 1u) != 0);
-      if (yv.heads == 0) {
-        if (tail || last) p.part_head[tile] = yv.v;  // the incoming run's part here
-      } else if (tail) {
-        st_cast<V>(p.out_dtype, p.out, base + yv.heads - 1, vop(p.init, yv.v));
-      } else if (last) {
-        p.tail_seg[tile] = base + yv.heads - 1;  // goes on past this tile
+    const uint32_t len = (uint32_t)(te - tb);
+    const int words = (int)((len + 31) / 32);
+    for (int w = tid; w < words; w += kThreads) {
+      const uint32_t hb = s_bits[w];
+      const uint32_t lo = (uint32_t)w * 32;
+      const uint32_t valid = len - lo >= 32 ? ~0u : ((1u << (len - lo)) - 1u);
+      uint32_t nxt = 0;  // whether the item after this word's last is a head
+      if (lo + 32 < len) nxt = s_bits[w + 1] & 1u;
+      else if (lo + 32 == len) nxt = s_head_te != 0;
+      uint32_t tails = ((hb >> 1) | (nxt << 31)) & valid;
+      if (len - lo < 32 && s_head_te) tails |= 1u << (len - 1 - lo);  // the tile's last item
+      if (p.out_keys)
+        for (uint32_t b = hb & valid; b; b &= b - 1) {
+          const uint32_t pos = lo + (uint32_t)(__ffs(b) - 1);
+          st_raw_bits(p.out_keys, base + stage[pos].heads - 1, p.out_key_esize,
+                      src_load_bits(p.keys, tb + pos));
+        }
+      for (uint32_t b = tails; b; b &= b - 1) {
+        const uint32_t pos = lo + (uint32_t)(__ffs(b) - 1);
+        const T yv = stage[pos];
+        if (yv.heads == 0) p.part_head[tile] = yv.v;  // the incoming run ends here
+        else st_cast<V>(p.out_dtype, p.out, base + yv.heads - 1, vop(p.init, yv.v));
       }
-      if (last) p.part_tail[tile] = yv.v;
+    }
+    if (tid == 0) {
+      const T yl = stage[len - 1];
+      p.part_tail[tile] = yl.v;
+      if (yl.heads == 0) p.part_head[tile] = yl.v;  // no head in the tile: all of it
+      else if (!s_head_te) p.tail_seg[tile] = base + yl.heads - 1;  // goes on past this tile
     }
     __shared__ uint32_t s_fp;  // the tile's first head
     if (tid == 0) s_fp = (uint32_t)(te - tb);
